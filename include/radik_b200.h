@@ -1,0 +1,113 @@
+/* radik_b200.h -- C ABI of the B200 radix top-k selection library.
+ *
+ * Drop-in boundary for RadiK's batched radix top-k (leefige/radik,
+ * radik/RadixSelect/topk_radixselect.h).  Plain pointers and sizes only; no
+ * C++ types cross it and no exception escapes it.  Every entry point returns a
+ * radik_status code (0 = success).  Launches are asynchronous on the given
+ * stream; device-side failures are reported by radik_get_status().
+ *
+ * Values: fp32, fp16 or bf16 (radik_dtype).  Indices: int32 by default,
+ * int64 with RADIK_IDX64 (applies to idx_in and idx_out together, as RadiK's
+ * single IdxType template parameter does).
+ */
+#ifndef RADIK_B200_H_
+#define RADIK_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Value types (RadiK: ValType = float / half; bf16 is declared by RadiK,
+ * radik/RadixSelect/utils.cuh:11-14, but cannot build there). */
+enum radik_dtype { RADIK_F32 = 0, RADIK_F16 = 1, RADIK_BF16 = 2 };
+
+/* Flags: RadiK's template parameters and needSorting as run-time bits
+ * (topk_radixselect.h:59-70). */
+#define RADIK_LARGEST 1u    /* LARGEST: top-k largest (else smallest)           */
+#define RADIK_SORTED 2u     /* needSorting: sort each row's k outputs           */
+#define RADIK_ASCEND 4u     /* ASCEND: sorted order ascending (else descending) */
+#define RADIK_WITHSCALE 8u  /* WITHSCALE: order by x - x[row start]             */
+#define RADIK_WITHIDXIN 16u /* WITHIDXIN: emit idx_in[row_off + pos]            */
+#define RADIK_IDX64 32u     /* idx_in / idx_out are int64 (else int32)          */
+
+enum radik_status {
+  RADIK_OK = 0,
+  RADIK_EINVAL = 1,      /* bad argument (RadiK throws std::runtime_error)      */
+  RADIK_EWORKSPACE = 2,  /* workspace null or too small (topk_radixselect.h:77) */
+  RADIK_ECUDA = 3,       /* a CUDA runtime call failed (error_check.hpp:14-58)  */
+  RADIK_ETIMEOUT = 4,    /* a bounded device wait gave up                       */
+  RADIK_EINTERNAL = 5,   /* the device reported an inconsistent selection       */
+  RADIK_ENOTSUP = 6      /* combination not supported                           */
+};
+
+/* Row descriptor of the uneven batched form: row r reads n values at
+ * val_in[in_off ..) (and idx_in[in_off ..) with RADIK_WITHIDXIN) and writes k
+ * results at val_out/idx_out[out_off ..). */
+typedef struct radik_row_desc {
+  int64_t in_off;
+  int64_t out_off;
+  int32_t n;
+  int32_t k;
+} radik_row_desc;
+
+/* Replaces getRadixSelectLWorkSpaceSize<ValType>(K, n, taskNum, &bytes)
+ * (radik/RadixSelect/topk_radixselect.h:22-33): bytes of device workspace for
+ * radik_topk() on task_num rows of at most n_max values.  flags must carry
+ * RADIK_SORTED if the calls will sort (a larger scratch is reserved for
+ * k > 16384). */
+int radik_get_workspace_size(int dtype, uint32_t flags, int K, int n_max, int task_num, size_t* bytes);
+
+/* Replaces topKRadixSelectL<IdxType, LARGEST, ASCEND, WITHSCALE, WITHIDXIN,
+ * ValType>(valIn, idxIn, valOut, idxOut, workSpace, taskLen, taskNum, K,
+ * stream, needSorting) (radik/RadixSelect/topk_radixselect.h:59-70).
+ *   val_in       device, the task_num rows back to back (no padding)
+ *   idx_in       device, same layout, only read with RADIK_WITHIDXIN
+ *   val_out/idx_out  device, task_num x K, row r at r * K
+ *   task_len     HOST array of task_num row lengths (as in RadiK)
+ * Rows shorter than K fill slots [n, K) with index -1 and value 0 (RadiK does
+ * this on its sorted path, topk_radixselect.h:312-320).  Ties at the k-th
+ * value go to the lowest positions.  Unsorted output order is unspecified. */
+int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+               void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K,
+               void* stream);
+
+/* Workspace for radik_topk_rows(): task_num rows, total_n values in all,
+ * the longest n_max, the largest k k_max.  The same four bounds must be
+ * passed to radik_topk_rows(), which lays the workspace out from them. */
+int radik_get_workspace_size_rows(int dtype, uint32_t flags, int task_num, int64_t total_n, int n_max, int k_max,
+                                  size_t* bytes);
+
+/* Uneven batched one-launch form: per-row n and k from a DEVICE array of
+ * descriptors.  No host synchronisation and no host-side planning, so the
+ * call can be captured in a CUDA graph.  Semantics per row as radik_topk.
+ * total_n / n_max / k_max are upper bounds of the rows' sum of n, largest n
+ * and largest k (the values given to radik_get_workspace_size_rows); a
+ * descriptor set that exceeds them is rejected on the device
+ * (radik_get_status -> RADIK_EWORKSPACE).  RadiK's batch has one K for all
+ * rows (topk_radixselect.h:107-110); this form stands beside the plain one. */
+int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                    void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                    int task_num, int64_t total_n, int n_max, int k_max, void* stream);
+
+/* Synchronises the stream and returns the status of the last call made with
+ * this workspace (RADIK_OK, RADIK_ETIMEOUT, RADIK_EINTERNAL, RADIK_EWORKSPACE).
+ * device_bits (nullable) receives the raw device status word. */
+int radik_get_status(void* workspace, void* stream, int* device_bits);
+
+/* Human-readable text of a radik_status code. */
+const char* radik_strerror(int status);
+
+/* Text of the last error raised on the calling host thread. */
+const char* radik_last_error(void);
+
+/* Library version as 10000 * major + 100 * minor + patch. */
+int radik_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RADIK_B200_H_ */

@@ -1,0 +1,237 @@
+"""radik_b200 -- B200-native radix top-k selection.
+
+Python host mirror of RadiK's entry points (leefige/radik,
+radik/RadixSelect/topk_radixselect.h) over the library's C ABI
+(include/radik_b200.h).  PyTorch supplies device memory and streams; the
+selection itself runs in the in-tree CUDA library ``libradik_b200.so``.  There
+is no fallback: if the library is missing, importing the bindings raises.
+
+Reference mapping:
+  getRadixSelectLWorkSpaceSize<ValType>(K, n, taskNum, &bytes)
+      -> get_radix_select_l_workspace_size(dtype, K, n, task_num, ...)
+  topKRadixSelectL<IdxType, LARGEST, ASCEND, WITHSCALE, WITHIDXIN>(
+      valIn, idxIn, valOut, idxOut, workSpace, taskLen, taskNum, K, stream,
+      needSorting)
+      -> topk_radix_select_l(val_in, idx_in, val_out, idx_out, workspace,
+                             task_len, K, largest=, ascend=, with_scale=,
+                             with_idx_in=, need_sorting=, stream=)
+  std::runtime_error -> RadikError
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libradik_b200.so")
+
+F32, F16, BF16 = 0, 1, 2
+LARGEST, SORTED, ASCEND, WITHSCALE, WITHIDXIN, IDX64 = 1, 2, 4, 8, 16, 32
+
+OK, EINVAL, EWORKSPACE, ECUDA, ETIMEOUT, EINTERNAL, ENOTSUP = range(7)
+
+
+class RadikError(RuntimeError):
+    """A non-zero status from the library (RadiK raises std::runtime_error)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"radik_b200 error {code}: {msg}")
+        self.code = code
+
+
+class RowDesc(ctypes.Structure):
+    _fields_ = [("in_off", ctypes.c_int64), ("out_off", ctypes.c_int64), ("n", ctypes.c_int32), ("k", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"radik_b200: {LIB_PATH} is missing; build it with `python -m radik_b200.build` "
+            "(there is no CPU fallback)"
+        )
+    L = ctypes.CDLL(LIB_PATH)
+    vp, u32, i32, i64, sz = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int64, ctypes.c_size_t
+    L.radik_get_workspace_size.argtypes = [i32, u32, i32, i32, i32, ctypes.POINTER(sz)]
+    L.radik_get_workspace_size_rows.argtypes = [i32, u32, i32, i64, i32, i32, ctypes.POINTER(sz)]
+    L.radik_topk.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp]
+    L.radik_topk_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp]
+    L.radik_get_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
+    L.radik_strerror.argtypes = [i32]
+    L.radik_strerror.restype = ctypes.c_char_p
+    L.radik_last_error.argtypes = []
+    L.radik_last_error.restype = ctypes.c_char_p
+    L.radik_version.argtypes = []
+    for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
+                 "radik_get_status", "radik_version"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(code: int) -> None:
+    if code != OK:
+        msg = lib().radik_last_error().decode(errors="replace")
+        raise RadikError(code, msg or lib().radik_strerror(code).decode())
+
+
+def dtype_code(torch_dtype) -> int:
+    import torch
+
+    m = {torch.float32: F32, torch.float16: F16, torch.bfloat16: BF16}
+    if torch_dtype not in m:
+        raise RadikError(EINVAL, f"unsupported value dtype {torch_dtype}")
+    return m[torch_dtype]
+
+
+def make_flags(largest: bool = True, sorted: bool = False, ascend: Optional[bool] = None,
+               with_scale: bool = False, with_idx_in: bool = False, idx64: bool = False) -> int:
+    """Flag bits; ascend defaults to the natural order (descending for largest)."""
+    if ascend is None:
+        ascend = not largest
+    f = 0
+    f |= LARGEST if largest else 0
+    f |= SORTED if sorted else 0
+    f |= ASCEND if ascend else 0
+    f |= WITHSCALE if with_scale else 0
+    f |= WITHIDXIN if with_idx_in else 0
+    f |= IDX64 if idx64 else 0
+    return f
+
+
+def get_radix_select_l_workspace_size(dtype: int, K: int, n: int, task_num: int, flags: int = SORTED) -> int:
+    """Bytes of workspace for topk_radix_select_l (getRadixSelectLWorkSpaceSize)."""
+    out = ctypes.c_size_t(0)
+    _check(lib().radik_get_workspace_size(dtype, flags, K, n, task_num, ctypes.byref(out)))
+    return out.value
+
+
+def get_rows_workspace_size(dtype: int, task_num: int, total_n: int, n_max: int, k_max: int, flags: int = SORTED) -> int:
+    out = ctypes.c_size_t(0)
+    _check(lib().radik_get_workspace_size_rows(dtype, flags, task_num, total_n, n_max, k_max, ctypes.byref(out)))
+    return out.value
+
+
+def _stream_handle(stream) -> Optional[int]:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+def topk_radix_select_l(val_in, idx_in, val_out, idx_out, workspace, task_len: Sequence[int], K: int, *,
+                        largest: bool, ascend: bool, with_scale: bool = False, with_idx_in: bool = False,
+                        need_sorting: bool = True, stream=None, idx64: Optional[bool] = None) -> None:
+    """Mirror of topKRadixSelectL (topk_radixselect.h:59-70) on torch CUDA tensors.
+
+    val_in holds the rows back to back; val_out/idx_out are task_num x K;
+    task_len is a host sequence of row lengths.  Asynchronous on ``stream``.
+    """
+    import torch
+
+    if workspace is None:
+        raise RadikError(EWORKSPACE, "radix topk: workspace should not be null")
+    if idx64 is None:
+        idx64 = idx_out.dtype == torch.int64
+    flags = make_flags(largest, need_sorting, ascend, with_scale, with_idx_in, idx64)
+    n = len(task_len)
+    arr = (ctypes.c_int * max(n, 1))(*[int(x) for x in task_len])
+    _check(lib().radik_topk(
+        dtype_code(val_in.dtype), flags, val_in.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+        val_out.data_ptr(), idx_out.data_ptr(), workspace.data_ptr(), workspace.numel() * workspace.element_size(),
+        arr, n, int(K), _stream_handle(stream)))
+
+
+def status(workspace, stream=None) -> int:
+    """Synchronise ``stream`` and raise RadikError if the last call failed on the device."""
+    bits = ctypes.c_int(0)
+    _check(lib().radik_get_status(workspace.data_ptr(), _stream_handle(stream), ctypes.byref(bits)))
+    return bits.value
+
+
+def topk(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bool = True, sorted: bool = False,
+         ascend: Optional[bool] = None, with_scale: bool = False, idx_in=None, idx64: bool = False,
+         workspace=None, stream=None, check: bool = True) -> Tuple["object", "object"]:
+    """Batched top-k of torch CUDA values.
+
+    values: 2-D (rows of equal length) or 1-D with ``lengths`` (rows back to
+    back).  Returns (vals[B, k], idx[B, k]); indices are positions in each row
+    (or idx_in entries).  ``check`` synchronises and raises on a device error.
+    """
+    import torch
+
+    if values.dim() == 2:
+        B, n = values.shape
+        lengths = [n] * B
+        flat = values.contiguous().view(-1)
+    else:
+        if lengths is None:
+            lengths = [values.numel()]
+        flat = values.contiguous()
+        B = len(lengths)
+    flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
+    dt = dtype_code(values.dtype)
+    n_max = max(lengths) if lengths else 0
+    if workspace is None:
+        ws_bytes = get_radix_select_l_workspace_size(dt, k, n_max, B, flags)
+        workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=values.device)
+    vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
+    idx = torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device)
+    arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
+    _check(lib().radik_topk(dt, flags, flat.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+                            vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                            arr, B, int(k), _stream_handle(stream)))
+    if check:
+        status(workspace, stream)
+    return vals, idx
+
+
+def topk_rows(values, rows, *, largest: bool = True, sorted: bool = False, ascend: Optional[bool] = None,
+              with_scale: bool = False, idx_in=None, idx64: bool = False, total_out: Optional[int] = None,
+              bounds: Optional[Tuple[int, int, int]] = None, workspace=None, stream=None, check: bool = True):
+    """Uneven batched one-launch top-k.
+
+    rows: host list of (in_off, out_off, n, k) or a device uint8/int64 tensor
+    holding radik_row_desc records.  Returns flat (vals, idx) of total_out
+    slots.  bounds = (total_n, n_max, k_max) for the workspace layout.
+    """
+    import torch
+
+    dev = values.device
+    if isinstance(rows, torch.Tensor):
+        desc = rows
+        if bounds is None or total_out is None:
+            raise RadikError(EINVAL, "device descriptors need bounds and total_out")
+        B = desc.numel() * desc.element_size() // ctypes.sizeof(RowDesc)
+    else:
+        B = len(rows)
+        host = (RowDesc * max(B, 1))()
+        for i, (a, b, n, kk) in enumerate(rows):
+            host[i] = RowDesc(int(a), int(b), int(n), int(kk))
+        raw = torch.frombuffer(bytearray(bytes(host)), dtype=torch.uint8)
+        desc = raw.to(dev)
+        if bounds is None:
+            bounds = (sum(r[2] for r in rows), max((r[2] for r in rows), default=0), max((r[3] for r in rows), default=0))
+        if total_out is None:
+            total_out = max((r[1] + r[3] for r in rows), default=0)
+    total_n, n_max, k_max = bounds
+    flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
+    dt = dtype_code(values.dtype)
+    if workspace is None:
+        workspace = torch.empty(get_rows_workspace_size(dt, B, total_n, n_max, k_max, flags), dtype=torch.uint8, device=dev)
+    vals = torch.empty(max(total_out, 1), dtype=values.dtype, device=dev)
+    idx = torch.empty(max(total_out, 1), dtype=torch.int64 if idx64 else torch.int32, device=dev)
+    _check(lib().radik_topk_rows(dt, flags, values.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+                                 vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                 desc.data_ptr(), B, int(total_n), int(n_max), int(k_max), _stream_handle(stream)))
+    if check:
+        status(workspace, stream)
+    return vals[:total_out], idx[:total_out]

@@ -1,0 +1,72 @@
+"""Build recipe for the in-tree CUDA library (sm_100a) and the test checkers.
+
+``build()`` compiles radik_b200/libradik_b200.so with nvcc for sm_100a and, via
+oracle/Makefile, the CPU oracle (and the reference RadiK wrapper when the
+reference sources are present).  The .so files stay in the tree so they ship
+with it; nothing is installed into site-packages.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libradik_b200.so")
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("radik_engine.cu", "radik_api.cu")]
+HEADERS = [os.path.join(HERE, "csrc", "radik_common.cuh"), os.path.join(ROOT, "include", "radik_b200.h")]
+
+NVCC_FLAGS = [
+    "-O3",
+    "-std=c++17",
+    "-gencode",
+    "arch=compute_100a,code=sm_100a",
+    "-lineinfo",
+    "-Xcompiler",
+    "-fPIC",
+    "-shared",
+]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build radik_b200")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> str:
+    if force or _stale(LIB, SOURCES + HEADERS):
+        cmd = [_nvcc(), *NVCC_FLAGS, "-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *SOURCES]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_oracle(verbose: bool = False) -> None:
+    make = shutil.which("make")
+    if make is None:
+        raise RuntimeError("make not found")
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.run([make, "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True, stdout=out)
+
+
+def build(force: bool = False, verbose: bool = False) -> None:
+    build_library(force=force, verbose=verbose)
+    build_oracle(verbose=verbose)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,354 @@
+// radik_api.cu -- host side of the C ABI declared in include/radik_b200.h.
+//
+// Each call: validate, lay out the caller's workspace, clear the per-call
+// state with one cudaMemsetAsync, and launch the selection engine (plus the
+// one-CTA planning kernel when the rows are not uniform).  No host
+// synchronisation, unlike RadiK's two cudaStreamSynchronize per call
+// (radik/RadixSelect/topk_radixselect.h:157,195).
+
+#include "radik_common.cuh"
+#include "radik_b200.h"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace radik {
+
+cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* chunk_row,
+                        Header* hdr, int64_t nc_cap, int64_t cand_cap_total, int64_t sort_cap_total, int grid,
+                        cudaStream_t stream);
+
+namespace {
+
+constexpr uint32_t kKnownFlags = kFlagLargest | kFlagSorted | kFlagAscend | kFlagWithScale | kFlagWithIdxIn | kFlagIdx64;
+constexpr int kSlots = 64;             // level-1 histogram ring slots
+constexpr int kMinCH = 4096;           // chunk length bounds (elements)
+constexpr int kMaxCH = 65536;
+constexpr uint32_t kSpinLimit = 1u << 23;
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(RADIK_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int sm_count() {
+  static std::mutex mu;
+  static int cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  if (dev >= 0 && dev < 64) cache[dev] = sms;
+  return sms;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Layout {
+  size_t hdr, rs, slot_gen, hist, zero_end;
+  size_t plans, chunk_row, large, descs, cand, sort, total;
+};
+
+Layout make_layout(int64_t B, int64_t nc_cap, int64_t cand_cap, int64_t sort_cap) {
+  Layout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += align256(bytes);
+    return o;
+  };
+  L.hdr = take(sizeof(Header));
+  L.rs = take((size_t)B * sizeof(RowState));
+  L.slot_gen = take((size_t)kSlots * 4);
+  L.hist = take((size_t)kSlots * ((size_t)1 << kMaxD1) * 4);
+  L.zero_end = off;
+  L.plans = take((size_t)B * sizeof(RowPlan));
+  L.chunk_row = take((size_t)nc_cap * 4);
+  L.large = take((size_t)B * 4);
+  L.descs = take((size_t)B * sizeof(RowDesc));
+  L.cand = take((size_t)cand_cap * 8);
+  L.sort = take((size_t)sort_cap * 8);
+  L.total = off;
+  return L;
+}
+
+struct Bounds {
+  int64_t nc, cand, sort;
+};
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
+  Bounds b{};
+  b.nc = B * std::max<int64_t>(1, ceil_div(n_max, kMinCH));
+  b.cand = is_smem_row((int32_t)n_max) ? 0 : B * (int64_t)cand_capacity((int32_t)n_max);
+  const int64_t kk = std::min(n_max, K);
+  b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? B * 2 * kk : 0;
+  return b;
+}
+
+Bounds bounds_rows(int64_t B, int64_t total_n, int64_t n_max, int64_t k_max, uint32_t flags) {
+  Bounds b{};
+  b.nc = total_n / kMinCH + B;
+  b.cand = std::min(total_n, B * (int64_t)kCapSB) + total_n / 8 + B;
+  const int64_t kk = std::min(n_max, k_max);
+  b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * std::min(total_n, B * k_max) : 0;
+  return b;
+}
+
+int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  if (!v || !*v) return dflt;
+  return std::atoi(v);
+}
+
+// Tunables: chunk length and first-digit width.  The defaults aim at about
+// four chunks per CTA so the work queue balances, with chunks of 4K..64K
+// elements, and a 14-bit first digit (16384 bins, 64 KB of shared memory):
+// for i.i.d. fp32 rows the selected bin then holds about n/64 keys, which a
+// finisher resolves in shared memory.  RADIK_CH / RADIK_D1 override them
+// (tuning sweeps).
+struct Config {
+  int CH, D1;
+};
+
+Config choose_config(int64_t multi_elems, int grid) {
+  Config c{};
+  const int64_t target = std::max<int64_t>(1, multi_elems / ((int64_t)grid * 4));
+  int ch = kMinCH;
+  while (ch < kMaxCH && ch * 2 <= target) ch *= 2;
+  c.CH = ch;
+  c.D1 = kMaxD1;
+  const int ech = env_int("RADIK_CH", 0);
+  if (ech >= kMinCH && ech <= (1 << 24) && (ech % 16) == 0) c.CH = ech;
+  const int ed1 = env_int("RADIK_D1", 0);
+  if (ed1 >= kMinD1 && ed1 <= kMaxD1) c.D1 = ed1;
+  return c;
+}
+
+int check_common(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+                 void* ws) {
+  if (dtype != kF32 && dtype != kF16 && dtype != kBF16) return fail(RADIK_EINVAL, "radik: unknown dtype");
+  if (flags & ~kKnownFlags) return fail(RADIK_EINVAL, "radik: unknown flag bits");
+  if (!val_in || !val_out || !idx_out) return fail(RADIK_EINVAL, "radik: null input/output pointer");
+  if ((flags & kFlagWithIdxIn) && !idx_in) return fail(RADIK_EINVAL, "radik: RADIK_WITHIDXIN needs idx_in");
+  if (!ws) return fail(RADIK_EWORKSPACE, "radik: workspace should not be null");
+  if ((reinterpret_cast<uintptr_t>(ws) & 255u) != 0) return fail(RADIK_EWORKSPACE, "radik: workspace must be 256-byte aligned");
+  const uintptr_t es = (uintptr_t)elem_bytes(dtype);
+  if ((reinterpret_cast<uintptr_t>(val_in) % es) || (reinterpret_cast<uintptr_t>(val_out) % es))
+    return fail(RADIK_EINVAL, "radik: value pointers must be aligned to the element size");
+  return RADIK_OK;
+}
+
+EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, void* idx_out, uint8_t* ws,
+                         const Layout& L, int B, const Config& c, uint32_t flags) {
+  EngineParams p{};
+  p.val_in = val_in;
+  p.idx_in = idx_in;
+  p.val_out = val_out;
+  p.idx_out = idx_out;
+  p.rs = reinterpret_cast<RowState*>(ws + L.rs);
+  p.hist_ring = reinterpret_cast<uint32_t*>(ws + L.hist);
+  p.slot_gen = reinterpret_cast<uint32_t*>(ws + L.slot_gen);
+  p.hdr = reinterpret_cast<Header*>(ws + L.hdr);
+  p.large_list = reinterpret_cast<int32_t*>(ws + L.large);
+  p.cand = reinterpret_cast<uint64_t*>(ws + L.cand);
+  p.sort_scratch = reinterpret_cast<uint64_t*>(ws + L.sort);
+  p.B = B;
+  p.CH = c.CH;
+  p.D1 = c.D1;
+  p.S = kSlots;
+  p.flags = flags;
+  p.spin_limit = kSpinLimit;
+  return p;
+}
+
+size_t zero_bytes(const Layout& L, const Config& c) {
+  return L.hist + (size_t)kSlots * ((size_t)1 << c.D1) * 4;
+}
+
+}  // namespace
+}  // namespace radik
+
+using namespace radik;
+
+extern "C" {
+
+int radik_version(void) { return 100; }
+
+const char* radik_last_error(void) { return g_last_error.c_str(); }
+
+const char* radik_strerror(int status) {
+  switch (status) {
+    case RADIK_OK: return "success";
+    case RADIK_EINVAL: return "invalid argument";
+    case RADIK_EWORKSPACE: return "workspace null or too small";
+    case RADIK_ECUDA: return "CUDA runtime error";
+    case RADIK_ETIMEOUT: return "a bounded device wait timed out";
+    case RADIK_EINTERNAL: return "internal selection error";
+    case RADIK_ENOTSUP: return "unsupported combination";
+    default: return "unknown status";
+  }
+}
+
+int radik_get_workspace_size(int dtype, uint32_t flags, int K, int n_max, int task_num, size_t* bytes) {
+  if (!bytes) return fail(RADIK_EINVAL, "radik: bytes is null");
+  if (dtype != kF32 && dtype != kF16 && dtype != kBF16) return fail(RADIK_EINVAL, "radik: unknown dtype");
+  if (K < 0 || n_max < 0 || task_num < 0) return fail(RADIK_EINVAL, "radik: negative size");
+  const Bounds b = bounds_uniform(std::max(task_num, 1), n_max, K, flags);
+  *bytes = make_layout(std::max(task_num, 1), b.nc, b.cand, b.sort).total;
+  return RADIK_OK;
+}
+
+int radik_get_workspace_size_rows(int dtype, uint32_t flags, int task_num, int64_t total_n, int n_max, int k_max,
+                                  size_t* bytes) {
+  if (!bytes) return fail(RADIK_EINVAL, "radik: bytes is null");
+  if (dtype != kF32 && dtype != kF16 && dtype != kBF16) return fail(RADIK_EINVAL, "radik: unknown dtype");
+  if (task_num < 0 || total_n < 0 || n_max < 0 || k_max < 0) return fail(RADIK_EINVAL, "radik: negative size");
+  const Bounds b = bounds_rows(std::max(task_num, 1), total_n, n_max, k_max, flags);
+  *bytes = make_layout(std::max(task_num, 1), b.nc, b.cand, b.sort).total;
+  return RADIK_OK;
+}
+
+int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+               void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream_) {
+  int rc = check_common(dtype, flags, val_in, idx_in, val_out, idx_out, workspace);
+  if (rc) return rc;
+  if (task_num < 0 || K < 0) return fail(RADIK_EINVAL, "radik: negative task_num or K");
+  if (task_num == 0 || K == 0) return RADIK_OK;
+  if (!task_len) return fail(RADIK_EINVAL, "radik: task_len is null");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  const int B = task_num;
+  int n_max = 0;
+  bool uniform = true;
+  int64_t total_n = 0, multi_elems = 0;
+  for (int i = 0; i < B; ++i) {
+    const int n = task_len[i];
+    if (n < 0) return fail(RADIK_EINVAL, "radik: negative task length");
+    n_max = std::max(n_max, n);
+    uniform = uniform && n == task_len[0];
+    total_n += n;
+    if (!is_smem_row(n) && K < n) multi_elems += n;
+  }
+  if ((int64_t)B * K > ((int64_t)1 << 40)) return fail(RADIK_EINVAL, "radik: output too large");
+  const int grid = sm_count();
+  const Config cfg = choose_config(multi_elems, grid);
+  // exact needs of this call
+  int64_t nc = 0, cand = 0, sortn = 0, nch_max = 1;
+  for (int i = 0; i < B; ++i) {
+    const int n = task_len[i];
+    const bool multi = !is_smem_row(n) && K < n;
+    const bool all = !is_smem_row(n) && K >= n;
+    const int64_t nch = (multi || all) ? ceil_div(n, cfg.CH) : 1;
+    nch_max = std::max(nch_max, nch);
+    nc += nch;
+    if (multi) cand += cand_capacity(n);
+    const int64_t kk = std::min<int64_t>(n, K);
+    if ((flags & kFlagSorted) && kk > kCapSort) sortn += 2 * kk;
+  }
+  if (nc >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many chunks");
+  const Layout L = make_layout(B, nc, cand, sortn);
+  if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, cfg), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
+  if (uniform) {
+    const int n = task_len[0];
+    p.uniform = 1;
+    p.u_n = n;
+    p.u_k = K;
+    const bool multi = !is_smem_row(n) && K < n;
+    const bool all = !is_smem_row(n) && K >= n;
+    p.u_nch = (multi || all) ? (int32_t)ceil_div(n, cfg.CH) : 1;
+    p.u_cand_cap = multi ? cand_capacity(n) : 0;
+    const int64_t kk = std::min<int64_t>(n, K);
+    p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
+    p.u_smem_row = is_smem_row(n);
+    p.lag = (int32_t)std::max<int64_t>(nch_max, 2 * grid);
+  } else {
+    std::vector<RowDesc> d(B);
+    int64_t off = 0;
+    for (int i = 0; i < B; ++i) {
+      d[i].in_off = off;
+      d[i].out_off = (int64_t)i * K;
+      d[i].n = task_len[i];
+      d[i].k = K;
+      off += task_len[i];
+    }
+    RowDesc* dd = reinterpret_cast<RowDesc*>(ws + L.descs);
+    e = cudaMemcpyAsync(dd, d.data(), sizeof(RowDesc) * B, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
+    p.chunk_row = reinterpret_cast<int32_t*>(ws + L.chunk_row);
+    e = launch_plan(dd, B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
+                    reinterpret_cast<int32_t*>(ws + L.chunk_row), p.hdr, nc, cand, sortn, grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "plan launch");
+  }
+  e = launch_engine(dtype, p, grid, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+  return RADIK_OK;
+}
+
+int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                    void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                    int task_num, int64_t total_n, int n_max, int k_max, void* stream_) {
+  int rc = check_common(dtype, flags, val_in, idx_in, val_out, idx_out, workspace);
+  if (rc) return rc;
+  if (task_num < 0 || total_n < 0 || n_max < 0 || k_max < 0) return fail(RADIK_EINVAL, "radik: negative size");
+  if (task_num == 0) return RADIK_OK;
+  if (!rows) return fail(RADIK_EINVAL, "radik: rows is null");
+  static_assert(sizeof(radik_row_desc) == sizeof(RowDesc), "descriptor layout");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  const int B = task_num;
+  const Bounds b = bounds_rows(B, total_n, n_max, k_max, flags);
+  if (b.nc >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many chunks");
+  const Layout L = make_layout(B, b.nc, b.cand, b.sort);
+  if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
+  const int grid = sm_count();
+  const Config cfg = choose_config(total_n, grid);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, cfg), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
+  p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
+  p.chunk_row = reinterpret_cast<int32_t*>(ws + L.chunk_row);
+  // The chunk budget assumed kMinCH-long chunks; with the chosen CH the
+  // true count is smaller, so the bound still holds.
+  e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
+                  reinterpret_cast<int32_t*>(ws + L.chunk_row), p.hdr, b.nc, b.cand, b.sort, grid, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "plan launch");
+  e = launch_engine(dtype, p, grid, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+  return RADIK_OK;
+}
+
+int radik_get_status(void* workspace, void* stream_, int* device_bits) {
+  if (!workspace) return fail(RADIK_EWORKSPACE, "radik: workspace should not be null");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+  int32_t bits = 0;
+  e = cudaMemcpy(&bits, static_cast<uint8_t*>(workspace) + offsetof(Header, status), sizeof(bits),
+                 cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy status");
+  if (device_bits) *device_bits = bits;
+  if (bits & kStatusCapacity) return fail(RADIK_EWORKSPACE, "radik: rows exceed the workspace bounds");
+  if (bits & kStatusTimeout) return fail(RADIK_ETIMEOUT, "radik: a device wait timed out");
+  if (bits) return fail(RADIK_EINTERNAL, "radik: internal selection error");
+  return RADIK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+// radik_common.cuh -- types, flags and device helpers shared by the selection
+// engine (radik_engine.cu) and the C-ABI host side (radik_api.cu).
+//
+// Key space.  Every input value is mapped once to an unsigned "selection key"
+// in which smaller means better: the order-preserving image of the float
+// (negative: flip all bits, else flip the sign bit -- the same map as RadiK's
+// getBinId, radik/RadixSelect/utils.cuh:329-334), complemented for largest-k.
+// fp32 keys and every WITHSCALE key (the float difference x - s, RadiK's
+// ComputeT<half> = float, utils.cuh:96-101) are 32 bits wide; unscaled
+// fp16/bf16 keys are 16 bits wide.  Selection is over the 64-bit composite
+// (key << IB | position), IB = bits of the row's largest position, so ties
+// at the k-th key resolve to the lowest positions and the result is unique.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace radik {
+
+// ----------------------------------------------------------------------------
+// Public constants (mirrored in include/radik_b200.h)
+// ----------------------------------------------------------------------------
+enum : uint32_t {
+  kFlagLargest = 1u,     // top-k largest (else smallest)
+  kFlagSorted = 2u,      // sort each row's output
+  kFlagAscend = 4u,      // sorted order ascending (else descending)
+  kFlagWithScale = 8u,   // RadiK's adaptive scaling: order by x - x[0]
+  kFlagWithIdxIn = 16u,  // emit idx_in[row_off + pos] instead of pos
+  kFlagIdx64 = 32u,      // idx_in / idx_out are int64 (else int32)
+};
+enum : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
+
+// ----------------------------------------------------------------------------
+// Engine geometry
+// ----------------------------------------------------------------------------
+constexpr int kThreads = 1024;           // one CTA per SM, 32 warps
+constexpr int kWarps = kThreads / 32;
+constexpr int kCapSB = 24576;            // candidates a finisher resolves in smem
+constexpr int kSmemRowCap = 16384;       // rows this short are selected in smem
+constexpr int kCapSort = 16384;          // outputs a finisher sorts in smem
+constexpr int kMaxD1 = 14;               // widest first digit (64 KB smem hist)
+constexpr int kMinD1 = 8;
+constexpr int kSmemBytes = 196 * 1024;   // dynamic smem per CTA
+constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scratch
+
+// Row modes decided by the level-1 selection.
+enum : int32_t {
+  kModeNone = 0,
+  kModeFinal = 1,   // matched bin == remaining k: F emits better-or-matched
+  kModeSB = 2,      // matched bin fits a finisher's smem: F compacts into it
+  kModeCand = 3,    // matched bin compacted into the candidate region
+  kModeDefer = 4,   // matched bin too large: levels continue on the input
+  kModeAll = 5,     // k >= n: every element is selected
+};
+
+// Status bits written by the device (Header::status).
+enum : int32_t {
+  kStatusTimeout = 1,       // a bounded wait gave up
+  kStatusSelect = 2,        // a histogram did not hold k keys (internal)
+  kStatusCapacity = 4,      // workspace too small for the planned rows
+  kStatusOverflow = 8,      // a candidate region overflowed (internal)
+  kStatusLevels = 16,       // resolution did not converge (internal)
+};
+
+// Per-row plan (written by the planning kernel, read by the engine).
+struct alignas(16) RowPlan {
+  int64_t in_off;    // element offset of the row in val_in / idx_in
+  int64_t out_off;   // first output slot of the row
+  int64_t cand_off;  // first candidate entry of the row (8 B entries)
+  int64_t sort_off;  // first sort-scratch entry (8 B entries), -1 if none
+  int32_t n;         // row length
+  int32_t k;         // requested k
+  int32_t chunk0;    // first chunk id of the row in the phase-A item space
+  int32_t nch;       // number of chunks (1 for an smem row)
+  int32_t cand_cap;  // candidate region capacity (entries)
+  int32_t slot_use;  // ordinal among multi-chunk rows (hist ring), -1 = smem row
+  int32_t pad0, pad1;
+};
+static_assert(sizeof(RowPlan) == 64, "RowPlan layout");
+
+// Per-row state, zeroed before every call.
+struct alignas(16) RowState {
+  int32_t hticket;     // H chunks finished
+  int32_t fticket;     // F chunks finished
+  int32_t ready;       // level-1 selection published
+  int32_t mode;        // kMode*
+  int32_t krem;        // k still to take from the matched set
+  int32_t count;       // size of the matched set
+  int32_t out_count;   // output slots reserved so far
+  int32_t cand_count;  // candidate entries written
+  uint64_t prefix;     // composite prefix of the matched set
+  int32_t plen;        // its length in bits
+  int32_t done;        // row finished
+  int32_t pad[4];
+};
+static_assert(sizeof(RowState) == 64, "RowState layout");
+
+// Call header, zeroed before every call.
+struct alignas(16) Header {
+  uint32_t qhead;       // phase-A claim counter
+  uint32_t bar_count;   // grid barrier arrivals
+  uint32_t bar_gen;     // grid barrier generation
+  int32_t status;       // kStatus* bits
+  int32_t nlarge;       // rows handed to phase B
+  int32_t nc;           // chunks planned (phase-A items = 2 * nc)
+  int32_t lag;          // H-ahead-of-F distance in chunks
+  int32_t plan_error;   // planning failed (capacity)
+  int64_t cand_total;   // candidate entries planned
+  int64_t sort_total;   // sort-scratch entries planned
+  int32_t pad[52];
+};
+static_assert(sizeof(Header) == 256, "Header layout");
+
+// Row descriptor given to the planning kernel.
+struct alignas(8) RowDesc {
+  int64_t in_off;
+  int64_t out_off;
+  int32_t n;
+  int32_t k;
+};
+static_assert(sizeof(RowDesc) == 24, "RowDesc layout");
+
+// Everything the engine kernel needs.  Passed by value (__grid_constant__).
+struct EngineParams {
+  const void* val_in;
+  const void* idx_in;
+  void* val_out;
+  void* idx_out;
+  const RowPlan* plans;     // null in uniform mode
+  RowState* rs;
+  const int32_t* chunk_row; // null in uniform mode
+  uint32_t* hist_ring;      // S slots of (1 << D1) counters
+  uint32_t* slot_gen;       // S release counters
+  Header* hdr;
+  int32_t* large_list;      // B entries
+  uint64_t* cand;           // candidate entries (valbits << 32 | pos)
+  uint64_t* sort_scratch;   // merge-sort scratch
+  int32_t B;
+  int32_t CH;               // chunk length (elements), multiple of 16
+  int32_t D1;               // first digit width
+  int32_t S;                // hist ring slots
+  int32_t lag;              // requested lag (chunks)
+  uint32_t flags;
+  uint32_t spin_limit;      // iterations of a bounded wait
+  // uniform mode: every row has n = u_n, k = u_k, contiguous input,
+  // output at r * u_k.
+  int32_t uniform;
+  int32_t u_n;
+  int32_t u_k;
+  int32_t u_nch;
+  int32_t u_cand_cap;
+  int32_t u_smem_row;
+  int64_t u_sort_cap;       // sort-scratch entries per row (0 if none)
+};
+
+// ----------------------------------------------------------------------------
+// Host+device helpers
+// ----------------------------------------------------------------------------
+__host__ __device__ inline int key_bits(int dtype, uint32_t flags) {
+  return (dtype == kF32 || (flags & kFlagWithScale)) ? 32 : 16;
+}
+__host__ __device__ inline int elem_bytes(int dtype) { return dtype == kF32 ? 4 : 2; }
+__host__ __device__ inline int index_bits(int64_t n) {
+  int b = 1;
+  while (b < 32 && ((int64_t)1 << b) < n) ++b;
+  return b;
+}
+// Candidate region capacity of a row: enough for the smem finisher's set or
+// one eighth of the row, whichever is larger (never more than n).
+__host__ __device__ inline int32_t cand_capacity(int32_t n) {
+  int64_t a = n < kCapSB ? n : kCapSB;
+  int64_t b = ((int64_t)n + 7) / 8;
+  return (int32_t)(a > b ? a : b);
+}
+__host__ __device__ inline bool is_smem_row(int32_t n) { return n <= kSmemRowCap; }
+
+}  // namespace radik

@@ -152,6 +152,7 @@ def main():
     ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=0, help="override the row count (profiling a smaller case)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -175,6 +176,9 @@ def main():
     torch.cuda.set_device(dev)
 
     B, n, k, dts, sorted_, largest, desc = WORKLOADS[args.workload]
+    if args.rows > 0:
+        B = args.rows
+        desc = desc.replace("256 ", f"{B} ", 1)
 
     x = make_inputs(B, n, dts)
     tdtype = torch.float16 if dts == "f16" else torch.float32

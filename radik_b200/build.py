@@ -15,8 +15,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libradik_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("radik_engine.cu", "radik_api.cu")]
-HEADERS = [os.path.join(HERE, "csrc", "radik_common.cuh"), os.path.join(ROOT, "include", "radik_b200.h")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in (
+    "radik_engine_f32.cu", "radik_engine_f16.cu", "radik_engine_bf16.cu", "radik_plan.cu", "radik_api.cu")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("radik_common.cuh", "radik_engine.cuh")] + [
+    os.path.join(ROOT, "include", "radik_b200.h")]
+OBJ_DIR = os.path.join(ROOT, "_build")
 
 NVCC_FLAGS = [
     "-O3",
@@ -26,7 +29,6 @@ NVCC_FLAGS = [
     "-lineinfo",
     "-Xcompiler",
     "-fPIC",
-    "-shared",
 ]
 
 
@@ -45,13 +47,29 @@ def _stale(target: str, deps) -> bool:
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:
-    if force or _stale(LIB, SOURCES + HEADERS):
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *SOURCES]
+    """Compiles each translation unit in parallel, then links the .so."""
+    if not (force or _stale(LIB, SOURCES + HEADERS)):
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    nvcc = _nvcc()
+    inc = "-I" + os.path.join(ROOT, "include")
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, inc, "-c", "-o", obj, src]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        os.replace(LIB + ".tmp", LIB)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs],
+                   check=True)
+    os.replace(LIB + ".tmp", LIB)
     return LIB
 
 

@@ -19,9 +19,10 @@
 namespace radik {
 
 cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
-cudaError_t launch_plan(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* chunk_row,
-                        Header* hdr, int64_t nc_cap, int64_t cand_cap_total, int64_t sort_cap_total, int grid,
-                        cudaStream_t stream);
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* a_row,
+                        int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
+                        int64_t sort_cap_total, int grid, cudaStream_t stream);
+cudaError_t engine_max_grid(int dtype, uint32_t flags, int* grid);
 
 namespace {
 
@@ -41,27 +42,36 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(RADIK_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-int sm_count() {
+// Cooperative grid of the engine on the current device (one CTA per SM).
+int engine_grid(int dtype, uint32_t flags, int* grid) {
   static std::mutex mu;
-  static int cache[64] = {};
+  static int cache[64][2] = {};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  const int key = (flags & kFlagWithScale) ? 1 : 0;
   std::lock_guard<std::mutex> lock(mu);
-  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
-  int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  if (dev >= 0 && dev < 64) cache[dev] = sms;
-  return sms;
+  if (dev >= 0 && dev < 64 && cache[dev][key] > 0) {
+    *grid = cache[dev][key];
+    return RADIK_OK;
+  }
+  int g = 0;
+  e = engine_max_grid(dtype, flags, &g);
+  if (e != cudaSuccess) return cuda_fail(e, "engine occupancy");
+  if (g <= 0) return fail(RADIK_ECUDA, "radik: the engine does not fit on this device");
+  if (dev >= 0 && dev < 64) cache[dev][key] = g;
+  *grid = g;
+  return RADIK_OK;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
   size_t hdr, rs, slot_gen, hist, zero_end;
-  size_t plans, chunk_row, large, descs, cand, sort, total;
+  size_t plans, a_row, b_row, large, descs, pb_sb, cand, sort, total;
 };
 
-Layout make_layout(int64_t B, int64_t nc_cap, int64_t cand_cap, int64_t sort_cap) {
+Layout make_layout(int64_t B, int64_t na_cap, int64_t nb_cap, int64_t cand_cap, int64_t sort_cap) {
   Layout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -75,9 +85,11 @@ Layout make_layout(int64_t B, int64_t nc_cap, int64_t cand_cap, int64_t sort_cap
   L.hist = take((size_t)kSlots * ((size_t)1 << kMaxD1) * 4);
   L.zero_end = off;
   L.plans = take((size_t)B * sizeof(RowPlan));
-  L.chunk_row = take((size_t)nc_cap * 4);
+  L.a_row = take((size_t)na_cap * 4);
+  L.b_row = take((size_t)nb_cap * 4);
   L.large = take((size_t)B * 4);
   L.descs = take((size_t)B * sizeof(RowDesc));
+  L.pb_sb = take((size_t)kPhaseBSlots * kCapSB * 8);
   L.cand = take((size_t)cand_cap * 8);
   L.sort = take((size_t)sort_cap * 8);
   L.total = off;
@@ -85,15 +97,17 @@ Layout make_layout(int64_t B, int64_t nc_cap, int64_t cand_cap, int64_t sort_cap
 }
 
 struct Bounds {
-  int64_t nc, cand, sort;
+  int64_t na, nb, cand, sort;
 };
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
   Bounds b{};
-  b.nc = B * std::max<int64_t>(1, ceil_div(n_max, kMinCH));
-  b.cand = is_smem_row((int32_t)n_max) ? 0 : B * (int64_t)cand_capacity((int32_t)n_max);
+  const int64_t nch = std::max<int64_t>(1, ceil_div(n_max, kMinCH));
+  b.na = B * nch;
+  b.nb = B * nch;
+  b.cand = n_max > kCtaRowCap ? B * (int64_t)cand_capacity((int32_t)n_max) : 0;
   const int64_t kk = std::min(n_max, K);
   b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? B * 2 * kk : 0;
   return b;
@@ -101,7 +115,8 @@ Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
 
 Bounds bounds_rows(int64_t B, int64_t total_n, int64_t n_max, int64_t k_max, uint32_t flags) {
   Bounds b{};
-  b.nc = total_n / kMinCH + B;
+  b.na = total_n / kMinCH + B;
+  b.nb = total_n / kMinCH + B;
   b.cand = std::min(total_n, B * (int64_t)kCapSB) + total_n / 8 + B;
   const int64_t kk = std::min(n_max, k_max);
   b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * std::min(total_n, B * k_max) : 0;
@@ -166,6 +181,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.large_list = reinterpret_cast<int32_t*>(ws + L.large);
   p.cand = reinterpret_cast<uint64_t*>(ws + L.cand);
   p.sort_scratch = reinterpret_cast<uint64_t*>(ws + L.sort);
+  p.pb_sb = reinterpret_cast<uint64_t*>(ws + L.pb_sb);
   p.B = B;
   p.CH = c.CH;
   p.D1 = c.D1;
@@ -175,9 +191,13 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   return p;
 }
 
-size_t zero_bytes(const Layout& L, const Config& c) {
-  return L.hist + (size_t)kSlots * ((size_t)1 << c.D1) * 4;
-}
+size_t zero_bytes(const Layout& L) { return L.zero_end; }
+
+// How far A items run ahead of B items beyond what correctness needs.
+// Radix rows re-read their chunks in B items, so their A items run two grids
+// ahead and the re-reads hit L2; pre-filter rows read their chunks once and
+// only need their sample item done, so a short lead suffices.
+int64_t lag_floor(bool has_radix, int grid) { return has_radix ? 2 * (int64_t)grid : std::max(2, grid / 4); }
 
 }  // namespace
 }  // namespace radik
@@ -208,7 +228,7 @@ int radik_get_workspace_size(int dtype, uint32_t flags, int K, int n_max, int ta
   if (dtype != kF32 && dtype != kF16 && dtype != kBF16) return fail(RADIK_EINVAL, "radik: unknown dtype");
   if (K < 0 || n_max < 0 || task_num < 0) return fail(RADIK_EINVAL, "radik: negative size");
   const Bounds b = bounds_uniform(std::max(task_num, 1), n_max, K, flags);
-  *bytes = make_layout(std::max(task_num, 1), b.nc, b.cand, b.sort).total;
+  *bytes = make_layout(std::max(task_num, 1), b.na, b.nb, b.cand, b.sort).total;
   return RADIK_OK;
 }
 
@@ -218,7 +238,7 @@ int radik_get_workspace_size_rows(int dtype, uint32_t flags, int task_num, int64
   if (dtype != kF32 && dtype != kF16 && dtype != kBF16) return fail(RADIK_EINVAL, "radik: unknown dtype");
   if (task_num < 0 || total_n < 0 || n_max < 0 || k_max < 0) return fail(RADIK_EINVAL, "radik: negative size");
   const Bounds b = bounds_rows(std::max(task_num, 1), total_n, n_max, k_max, flags);
-  *bytes = make_layout(std::max(task_num, 1), b.nc, b.cand, b.sort).total;
+  *bytes = make_layout(std::max(task_num, 1), b.na, b.nb, b.cand, b.sort).total;
   return RADIK_OK;
 }
 
@@ -231,53 +251,52 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
   if (!task_len) return fail(RADIK_EINVAL, "radik: task_len is null");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   const int B = task_num;
-  int n_max = 0;
   bool uniform = true;
-  int64_t total_n = 0, multi_elems = 0;
+  int64_t multi_elems = 0;
   for (int i = 0; i < B; ++i) {
     const int n = task_len[i];
     if (n < 0) return fail(RADIK_EINVAL, "radik: negative task length");
-    n_max = std::max(n_max, n);
     uniform = uniform && n == task_len[0];
-    total_n += n;
-    if (!is_smem_row(n) && K < n) multi_elems += n;
+    const int kind = row_kind(n, K);
+    if (kind == kKindAll || kind == kKindGridPref || kind == kKindGridRadix) multi_elems += n;
   }
   if ((int64_t)B * K > ((int64_t)1 << 40)) return fail(RADIK_EINVAL, "radik: output too large");
-  const int grid = sm_count();
+  int grid = 0;
+  rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
   const Config cfg = choose_config(multi_elems, grid);
   // exact needs of this call
-  int64_t nc = 0, cand = 0, sortn = 0, nch_max = 1;
+  int64_t na = 0, nb = 0, cand = 0, sortn = 0, maxlag = 0;
+  bool has_radix = false;
   for (int i = 0; i < B; ++i) {
     const int n = task_len[i];
-    const bool multi = !is_smem_row(n) && K < n;
-    const bool all = !is_smem_row(n) && K >= n;
-    const int64_t nch = (multi || all) ? ceil_div(n, cfg.CH) : 1;
-    nch_max = std::max(nch_max, nch);
-    nc += nch;
-    if (multi) cand += cand_capacity(n);
+    const int kind = row_kind(n, K);
+    has_radix = has_radix || kind == kKindGridRadix;
+    const int64_t ra = row_na(kind, n, cfg.CH), rb = row_nb(kind, n, cfg.CH);
+    if (rb > 0) maxlag = std::max(maxlag, na + ra - nb);
+    na += ra;
+    nb += rb;
+    cand += row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     if ((flags & kFlagSorted) && kk > kCapSort) sortn += 2 * kk;
   }
-  if (nc >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many chunks");
-  const Layout L = make_layout(B, nc, cand, sortn);
+  if (na + nb >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many work items");
+  const Layout L = make_layout(B, na, nb, cand, sortn);
   if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
   uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, cfg), stream);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
   if (uniform) {
     const int n = task_len[0];
+    const int kind = row_kind(n, K);
     p.uniform = 1;
     p.u_n = n;
     p.u_k = K;
-    const bool multi = !is_smem_row(n) && K < n;
-    const bool all = !is_smem_row(n) && K >= n;
-    p.u_nch = (multi || all) ? (int32_t)ceil_div(n, cfg.CH) : 1;
-    p.u_cand_cap = multi ? cand_capacity(n) : 0;
+    p.u_cand_cap = row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
-    p.u_smem_row = is_smem_row(n);
-    p.lag = (int32_t)std::max<int64_t>(nch_max, 2 * grid);
+    p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(has_radix, grid));
   } else {
     std::vector<RowDesc> d(B);
     int64_t off = 0;
@@ -292,9 +311,10 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
     e = cudaMemcpyAsync(dd, d.data(), sizeof(RowDesc) * B, cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
     p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
-    p.chunk_row = reinterpret_cast<int32_t*>(ws + L.chunk_row);
-    e = launch_plan(dd, B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
-                    reinterpret_cast<int32_t*>(ws + L.chunk_row), p.hdr, nc, cand, sortn, grid, stream);
+    p.a_row = reinterpret_cast<int32_t*>(ws + L.a_row);
+    p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
+    e = launch_plan(dd, B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans), reinterpret_cast<int32_t*>(ws + L.a_row),
+                    reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, na, nb, cand, sortn, grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "plan launch");
   }
   e = launch_engine(dtype, p, grid, stream);
@@ -314,21 +334,25 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   cudaStream_t stream = static_cast<cudaStream_t>(stream_);
   const int B = task_num;
   const Bounds b = bounds_rows(B, total_n, n_max, k_max, flags);
-  if (b.nc >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many chunks");
-  const Layout L = make_layout(B, b.nc, b.cand, b.sort);
+  if (b.na + b.nb >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many work items");
+  const Layout L = make_layout(B, b.na, b.nb, b.cand, b.sort);
   if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
-  const int grid = sm_count();
+  int grid = 0;
+  rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
   const Config cfg = choose_config(total_n, grid);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, cfg), stream);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
   p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
-  p.chunk_row = reinterpret_cast<int32_t*>(ws + L.chunk_row);
-  // The chunk budget assumed kMinCH-long chunks; with the chosen CH the
-  // true count is smaller, so the bound still holds.
+  p.a_row = reinterpret_cast<int32_t*>(ws + L.a_row);
+  p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
+  // The item budget assumed kMinCH-long chunks; with the chosen CH the true
+  // count is smaller, so the bound still holds.
   e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
-                  reinterpret_cast<int32_t*>(ws + L.chunk_row), p.hdr, b.nc, b.cand, b.sort, grid, stream);
+                  reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, b.na, b.nb,
+                  b.cand, b.sort, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan launch");
   e = launch_engine(dtype, p, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "engine launch");

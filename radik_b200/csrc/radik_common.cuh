@@ -37,13 +37,29 @@ constexpr int kThreads = 1024;           // one CTA per SM, 32 warps
 constexpr int kWarps = kThreads / 32;
 constexpr int kCapSB = 24576;            // candidates a finisher resolves in smem
 constexpr int kSmemRowCap = 16384;       // rows this short are selected in smem
+constexpr int kCtaRowCap = 1 << 18;      // rows this short are selected by one CTA
 constexpr int kCapSort = 16384;          // outputs a finisher sorts in smem
 constexpr int kMaxD1 = 14;               // widest first digit (64 KB smem hist)
 constexpr int kMinD1 = 8;
+constexpr int kPrefRatio = 64;           // pre-filter rows with k * 64 <= n
+constexpr int kSampleMax = 16384;        // sampled keys per row (64 KB smem)
+constexpr int kSampleMin = 1024;
+constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
+constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)
 constexpr int kSmemBytes = 196 * 1024;   // dynamic smem per CTA
 constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scratch
 
-// Row modes decided by the level-1 selection.
+// Row kinds (a function of n and k only).
+enum : int32_t {
+  kKindEmpty = 0,      // k <= 0: nothing to do
+  kKindSmem = 1,       // n <= kSmemRowCap: one item, row held in smem
+  kKindCta = 2,        // n <= kCtaRowCap: one item, one CTA selects the row
+  kKindAll = 3,        // k >= n: chunk items copy the whole row
+  kKindGridPref = 4,   // large row, small k/n: sample item + filter chunks
+  kKindGridRadix = 5,  // large row, large k/n: histogram chunks + filter chunks
+};
+
+// Row modes decided after the first level.
 enum : int32_t {
   kModeNone = 0,
   kModeFinal = 1,   // matched bin == remaining k: F emits better-or-matched
@@ -70,19 +86,19 @@ struct alignas(16) RowPlan {
   int64_t sort_off;  // first sort-scratch entry (8 B entries), -1 if none
   int32_t n;         // row length
   int32_t k;         // requested k
-  int32_t chunk0;    // first chunk id of the row in the phase-A item space
-  int32_t nch;       // number of chunks (1 for an smem row)
+  int32_t a0;        // first A item of the row
+  int32_t b0;        // first B item of the row
   int32_t cand_cap;  // candidate region capacity (entries)
-  int32_t slot_use;  // ordinal among multi-chunk rows (hist ring), -1 = smem row
+  int32_t slot_use;  // ordinal among histogram rows (hist ring), -1 = none
   int32_t pad0, pad1;
 };
 static_assert(sizeof(RowPlan) == 64, "RowPlan layout");
 
 // Per-row state, zeroed before every call.
 struct alignas(16) RowState {
-  int32_t hticket;     // H chunks finished
-  int32_t fticket;     // F chunks finished
-  int32_t ready;       // level-1 selection published
+  int32_t hticket;     // A items finished
+  int32_t fticket;     // B items finished
+  int32_t ready;       // first-level decision published
   int32_t mode;        // kMode*
   int32_t krem;        // k still to take from the matched set
   int32_t count;       // size of the matched set
@@ -90,8 +106,11 @@ struct alignas(16) RowState {
   int32_t cand_count;  // candidate entries written
   uint64_t prefix;     // composite prefix of the matched set
   int32_t plen;        // its length in bits
-  int32_t done;        // row finished
-  int32_t pad[4];
+  uint32_t thresh;     // pre-filter threshold key
+  int32_t src;         // phase B source: 0 = the row, 1 = its candidates
+  int32_t src_len;     // entries in the phase-B source
+  int32_t final_pass;  // phase B: the next filter is the last
+  int32_t sb_count;    // phase B: entries compacted for the finisher
 };
 static_assert(sizeof(RowState) == 64, "RowState layout");
 
@@ -102,12 +121,14 @@ struct alignas(16) Header {
   uint32_t bar_gen;     // grid barrier generation
   int32_t status;       // kStatus* bits
   int32_t nlarge;       // rows handed to phase B
-  int32_t nc;           // chunks planned (phase-A items = 2 * nc)
-  int32_t lag;          // H-ahead-of-F distance in chunks
+  int32_t na;           // A items planned
+  int32_t nb;           // B items planned
+  int32_t lag;          // A-ahead-of-B distance in items
   int32_t plan_error;   // planning failed (capacity)
+  uint32_t pbhead;      // phase-B claim counter
   int64_t cand_total;   // candidate entries planned
   int64_t sort_total;   // sort-scratch entries planned
-  int32_t pad[52];
+  int32_t pad[50];
 };
 static_assert(sizeof(Header) == 256, "Header layout");
 
@@ -128,18 +149,20 @@ struct EngineParams {
   void* idx_out;
   const RowPlan* plans;     // null in uniform mode
   RowState* rs;
-  const int32_t* chunk_row; // null in uniform mode
-  uint32_t* hist_ring;      // S slots of (1 << D1) counters
+  const int32_t* a_row;     // A item -> row (null in uniform mode)
+  const int32_t* b_row;     // B item -> row (null in uniform mode)
+  uint32_t* hist_ring;      // S slots of (1 << kMaxD1) counters
   uint32_t* slot_gen;       // S release counters
   Header* hdr;
   int32_t* large_list;      // B entries
   uint64_t* cand;           // candidate entries (valbits << 32 | pos)
   uint64_t* sort_scratch;   // merge-sort scratch
+  uint64_t* pb_sb;          // phase-B smem-bound candidates, kPhaseBSlots x kCapSB
   int32_t B;
   int32_t CH;               // chunk length (elements), multiple of 16
-  int32_t D1;               // first digit width
+  int32_t D1;               // first digit width of histogram rows
   int32_t S;                // hist ring slots
-  int32_t lag;              // requested lag (chunks)
+  int32_t lag;              // uniform mode: A-ahead-of-B distance
   uint32_t flags;
   uint32_t spin_limit;      // iterations of a bounded wait
   // uniform mode: every row has n = u_n, k = u_k, contiguous input,
@@ -147,9 +170,7 @@ struct EngineParams {
   int32_t uniform;
   int32_t u_n;
   int32_t u_k;
-  int32_t u_nch;
   int32_t u_cand_cap;
-  int32_t u_smem_row;
   int64_t u_sort_cap;       // sort-scratch entries per row (0 if none)
 };
 
@@ -165,6 +186,25 @@ __host__ __device__ inline int index_bits(int64_t n) {
   while (b < 32 && ((int64_t)1 << b) < n) ++b;
   return b;
 }
+__host__ __device__ inline bool is_smem_row(int32_t n) { return n <= kSmemRowCap; }
+__host__ __device__ inline int row_kind(int32_t n, int32_t k) {
+  if (k <= 0) return kKindEmpty;
+  if (n <= kSmemRowCap) return kKindSmem;
+  if (k >= n) return kKindAll;
+  if (n <= kCtaRowCap) return kKindCta;
+  if ((int64_t)k * kPrefRatio <= (int64_t)n) return kKindGridPref;
+  return kKindGridRadix;
+}
+__host__ __device__ inline int32_t ceil_div32(int64_t a, int64_t b) { return (int32_t)((a + b - 1) / b); }
+// Items of a row: A items run first; B items of a row depend on all of its A items.
+__host__ __device__ inline int32_t row_na(int kind, int32_t n, int32_t CH) {
+  if (kind == kKindAll || kind == kKindGridRadix) return ceil_div32(n, CH);
+  return 1;
+}
+__host__ __device__ inline int32_t row_nb(int kind, int32_t n, int32_t CH) {
+  if (kind == kKindGridPref || kind == kKindGridRadix) return ceil_div32(n, CH);
+  return 0;
+}
 // Candidate region capacity of a row: enough for the smem finisher's set or
 // one eighth of the row, whichever is larger (never more than n).
 __host__ __device__ inline int32_t cand_capacity(int32_t n) {
@@ -172,6 +212,22 @@ __host__ __device__ inline int32_t cand_capacity(int32_t n) {
   int64_t b = ((int64_t)n + 7) / 8;
   return (int32_t)(a > b ? a : b);
 }
-__host__ __device__ inline bool is_smem_row(int32_t n) { return n <= kSmemRowCap; }
+__host__ __device__ inline int32_t row_cand_cap(int kind, int32_t n) {
+  return (kind == kKindGridPref || kind == kKindGridRadix) ? cand_capacity(n) : 0;
+}
+__host__ __device__ inline bool row_uses_hist(int kind) { return kind == kKindGridRadix; }
+// Pre-filter sample size (a power of two near n / 256, clamped) and the rank
+// of the sampled key used as the threshold: about twice the expected rank of
+// the k-th key in the sample plus a margin of 8, so that fewer than k keys
+// pass only with negligible probability for i.i.d. rows.
+__host__ __device__ inline int32_t sample_size(int32_t n) {
+  int32_t s = kSampleMin;
+  while (s < kSampleMax && (int64_t)s * 2 * 256 <= n) s *= 2;
+  return s;
+}
+__host__ __device__ inline int32_t sample_rank(int32_t n, int32_t k, int32_t S) {
+  const int64_t r = (2 * (int64_t)k * S + n - 1) / n + 8;
+  return (int32_t)(r < S ? r : S);
+}
 
 }  // namespace radik

@@ -1,0 +1,1562 @@
+// radik_engine.cu -- the B200 radix top-k selection engine.
+//
+// One cooperative persistent launch (one 1024-thread CTA per SM) selects every
+// row of a batch.  It replaces RadiK's chain of ~10 launches and 2 host syncs
+// per call (radik/RadixSelect/topk_radixselect.h:117-307).
+//
+// Phase A: a work queue of items claimed from one global counter.
+//   * smem rows (n <= 16K): one item loads the row into shared memory and
+//     selects it there (8-bit radix digits over the composite key).
+//   * CTA rows (n <= 256K): one item; one CTA samples the row, filters it
+//     against the sampled threshold into shared memory and resolves it, or
+//     runs radix levels over the row (second reads come from L2).
+//   * large rows with k * 64 <= n ("pre-filter" rows): a sample item picks a
+//     threshold key T (the r-th smallest of a strided sample, r about twice
+//     the expected rank of the k-th key plus a margin); then one read of the
+//     row (filter items, one per chunk) compacts the keys <= T into the row's
+//     candidate region.  This fuses RadiK's first histogram and candidate
+//     passes (countBinEx + selectCandidateEx, radixselect_l.cuh:173-408)
+//     and its final filter (:438-832) into a single read of the keys.
+//   * other large rows ("radix" rows): histogram items compute the first
+//     digit (14 bits) of each chunk in shared memory (countBinEx); the CTA
+//     finishing a row's last histogram item selects the bin (selectBin,
+//     radixselect_l.cuh:45-126) in the same kernel; filter items then re-read
+//     the chunks (from L2: they trail the histogram items by a lag) and emit
+//     keys of better bins and compact the selected bin.
+//   The CTA finishing a row's last item resolves the row's candidates in
+//   shared memory (RadiK's passes 2-3 and filter) and sorts the outputs
+//   (bitonicSort_*, bitonic_sort.cuh:195-553).
+// Phase B (after a grid barrier; empty for i.i.d. data): rows whose
+//   threshold missed, whose candidates exceed shared memory, or whose
+//   selected bin is huge (skewed / adversarial rows) run multi-CTA radix
+//   levels of 12-bit digits over their candidates or the row, with grid
+//   barriers between histogram, bin selection, filter and finish.
+//
+// Ties at the k-th key go to the lowest positions: selection is over the
+// composite (key << IB | position).  Every wait is bounded (spin_limit); a wait
+// that gives up sets a status bit and the kernel still exits.
+//
+// Queue order: A items (sample / histogram / single-item rows / copy chunks)
+// and B items (filter chunks) interleave after the first L A items; every B
+// item of a row comes after all A items of that row (L is planned so), so a
+// CTA that waits for a row's threshold or bin only waits for items already
+// claimed by running CTAs, and the smallest unfinished item always progresses.
+
+#pragma once
+
+#include "radik_common.cuh"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace radik {
+namespace dev {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// ----------------------------------------------------------------------------
+// PTX helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int32_t* p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Streaming 16-byte load of read-only input.
+__device__ __forceinline__ uint4 ld_stream16(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p));
+  return r;
+}
+__device__ __forceinline__ uint32_t ld_cg_u32(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ uint64_t ld_cg_u64(const uint64_t* p) {
+  return (uint64_t)__ldcg(reinterpret_cast<const unsigned long long*>(p));
+}
+
+__device__ __forceinline__ uint64_t shr64(uint64_t x, int s) { return s >= 64 ? 0ull : (x >> s); }
+
+// ----------------------------------------------------------------------------
+// Keys
+// ----------------------------------------------------------------------------
+template <int VT, bool SCALE>
+struct KT {
+  static constexpr int ES = VT == kF32 ? 4 : 2;            // element bytes
+  static constexpr int VEC = 16 / ES;                       // elements per 16 B
+  static constexpr int KB = (VT == kF32 || SCALE) ? 32 : 16;
+  static constexpr uint32_t KMASK = KB == 32 ? 0xFFFFFFFFu : 0xFFFFu;
+};
+
+template <int VT>
+__device__ __forceinline__ float to_float(uint32_t bits) {
+  if constexpr (VT == kF32) return __uint_as_float(bits);
+  else if constexpr (VT == kF16) return __half2float(__ushort_as_half((unsigned short)bits));
+  else return __uint_as_float(bits << 16);
+}
+
+__device__ __forceinline__ uint32_t ukey32(uint32_t u) {
+  return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);
+}
+__device__ __forceinline__ uint32_t ukey16(uint32_t u) {
+  return (u ^ ((u & 0x8000u) ? 0xFFFFu : 0x8000u)) & 0xFFFFu;
+}
+__device__ __forceinline__ uint32_t unkey32(uint32_t k) { return (k & 0x80000000u) ? (k ^ 0x80000000u) : ~k; }
+__device__ __forceinline__ uint32_t unkey16(uint32_t k) {
+  return ((k & 0x8000u) ? (k ^ 0x8000u) : (~k)) & 0xFFFFu;
+}
+
+// Selection key (smaller = better).  flip is 0 (smallest) or KMASK (largest).
+template <int VT, bool SCALE>
+__device__ __forceinline__ uint32_t sel_key(uint32_t bits, uint32_t flip, float scaler) {
+  if constexpr (SCALE) {
+    const float d = __fsub_rn(to_float<VT>(bits), scaler);
+    return ukey32(__float_as_uint(d)) ^ flip;
+  } else if constexpr (VT == kF32) {
+    return ukey32(bits) ^ flip;
+  } else {
+    return ukey16(bits) ^ flip;
+  }
+}
+
+// Output-order key (unscaled value order, direction by ASCEND) and inverse.
+template <int VT>
+__device__ __forceinline__ uint32_t out_key(uint32_t bits, bool ascend) {
+  if constexpr (VT == kF32) return ascend ? ukey32(bits) : ~ukey32(bits);
+  else return ascend ? ukey16(bits) : (~ukey16(bits) & 0xFFFFu);
+}
+template <int VT>
+__device__ __forceinline__ uint32_t out_key_inv(uint32_t k, bool ascend) {
+  if constexpr (VT == kF32) return unkey32(ascend ? k : ~k);
+  else return unkey16(ascend ? k : (~k & 0xFFFFu));
+}
+
+// ----------------------------------------------------------------------------
+// Shared-memory scratch at the tail of the dynamic allocation
+// ----------------------------------------------------------------------------
+struct Misc {
+  uint32_t hist256[256];
+  uint32_t scan[64];
+  int32_t next_q;
+  int32_t bcast;
+  int32_t bcast2;
+  uint32_t sel_bin, sel_cum, sel_cnt, sel_found;
+  uint32_t counter;
+  // row-state snapshot taken by thread 0 after an acquire
+  int32_t st_mode, st_krem, st_count, st_plen;
+  uint64_t st_prefix;
+  int32_t st_candn;
+  int32_t pad[7];
+  int32_t pbtab[200];  // phase-B row table (row ids, chunk counts, prefix)
+};
+static_assert(sizeof(Misc) <= kMiscBytes, "Misc too large");
+
+__device__ __forceinline__ Misc* misc_of(uint8_t* smem) {
+  return reinterpret_cast<Misc*>(smem + (kSmemBytes - kMiscBytes));
+}
+
+// ----------------------------------------------------------------------------
+// Block primitives
+// ----------------------------------------------------------------------------
+// Exclusive scan of one value per thread; *total gets the block sum.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* scan, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) scan[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = scan[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    scan[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t base = warp ? scan[warp - 1] : 0u;
+  if (total) *total = scan[kWarps - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+// Finds the bin b of h[0..NB) with cum(<b) < krem <= cum(<=b).
+// Result in m->sel_*; m->sel_found = 0 if the bins hold fewer than krem.
+template <bool GLOBAL>
+__device__ void block_select(const uint32_t* h, int NB, uint32_t krem, Misc* m) {
+  if (threadIdx.x == 0) m->sel_found = 0;
+  const int per = (NB + kThreads - 1) / kThreads;
+  const int lo = threadIdx.x * per;
+  const int hi = min(NB, lo + per);
+  uint32_t s = 0;
+  if ((per & 3) == 0) {
+    for (int i = lo; i < hi; i += 4) {
+      uint4 v;
+      if constexpr (GLOBAL) v = __ldcg(reinterpret_cast<const uint4*>(h + i));
+      else v = *reinterpret_cast<const uint4*>(h + i);
+      s += v.x + v.y + v.z + v.w;
+    }
+  } else {
+    for (int i = lo; i < hi; ++i) s += GLOBAL ? ld_cg_u32(h + i) : h[i];
+  }
+  const uint32_t ex = block_excl_scan(s, m->scan, nullptr);
+  if (lo < hi && ex < krem && krem <= ex + s) {
+    uint32_t run = ex;
+    for (int i = lo; i < hi; ++i) {
+      const uint32_t c = GLOBAL ? ld_cg_u32(h + i) : h[i];
+      if (run + c >= krem) {
+        m->sel_bin = (uint32_t)i;
+        m->sel_cum = run;
+        m->sel_cnt = c;
+        m->sel_found = 1;
+        break;
+      }
+      run += c;
+    }
+  }
+  __syncthreads();
+}
+
+// Shared-memory histogram increment, aggregated: the bin of the first valid
+// lane is added once with the count of lanes that share it, which turns a
+// heavily repeated key (constant-heavy rows) into one update per warp.  One
+// predicated atomic per lane.  All 32 lanes must call it together; returns
+// how many lanes shared the leader's bin.
+__device__ __forceinline__ int hist_add_agg(uint32_t* hist, uint32_t bin, bool valid) {
+  const unsigned vm = __ballot_sync(kFull, valid);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(vm) - 1;
+  const uint32_t lb = __shfl_sync(kFull, bin, leader & 31);
+  const bool same = valid && bin == lb;
+  const unsigned sm = __ballot_sync(kFull, same);
+  const uint32_t add = same ? (lane == leader ? (uint32_t)__popc(sm) : 0u) : (valid ? 1u : 0u);
+  if (add) atomicAdd(&hist[bin], add);
+  return __popc(sm);
+}
+
+// Histogram update for the e-th element of a 16-byte vector.  Element 0 goes
+// through the aggregated path and decides, per warp, whether the rest of the
+// vector does too (only when lanes repeat a bin); otherwise one plain atomic.
+__device__ __forceinline__ void hist_add(uint32_t* hist, uint32_t bin, bool valid, int e, bool& agg) {
+  if (e == 0) {
+    agg = hist_add_agg(hist, bin, valid) >= 3;
+  } else if (agg) {
+    hist_add_agg(hist, bin, valid);
+  } else if (valid) {
+    atomicAdd(&hist[bin], 1u);
+  }
+}
+
+// Bitonic sort of n (power of two, >= 2) uint64 keys in shared memory.
+__device__ inline void block_bitonic_sort(uint64_t* s, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < (n >> 1); i += kThreads) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const uint64_t a = s[lo], b = s[hi];
+        if ((a > b) == up) {
+          s[lo] = b;
+          s[hi] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Row context
+// ----------------------------------------------------------------------------
+struct RowCtx {
+  int64_t in_off, out_off, cand_off, sort_off;
+  int32_t n, k, a0, b0, na, nb, cand_cap, slot_use;
+  int32_t kind, IB;
+  uint32_t flip;
+  float scaler;
+};
+
+template <int VT, bool SCALE>
+__device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
+  RowCtx c;
+  if (p.uniform) {
+    c.n = p.u_n;
+    c.k = p.u_k;
+    c.in_off = (int64_t)r * p.u_n;
+    c.out_off = (int64_t)r * p.u_k;
+    c.kind = row_kind(c.n, c.k);
+    c.na = row_na(c.kind, c.n, p.CH);
+    c.nb = row_nb(c.kind, c.n, p.CH);
+    c.a0 = r * c.na;
+    c.b0 = r * c.nb;
+    c.cand_cap = p.u_cand_cap;
+    c.cand_off = (int64_t)r * p.u_cand_cap;
+    c.sort_off = p.u_sort_cap ? (int64_t)r * p.u_sort_cap : -1;
+    c.slot_use = row_uses_hist(c.kind) ? r : -1;
+  } else {
+    const RowPlan& pl = p.plans[r];
+    c.in_off = pl.in_off;
+    c.out_off = pl.out_off;
+    c.cand_off = pl.cand_off;
+    c.sort_off = pl.sort_off;
+    c.n = pl.n;
+    c.k = pl.k;
+    c.kind = row_kind(c.n, c.k);
+    c.na = row_na(c.kind, c.n, p.CH);
+    c.nb = row_nb(c.kind, c.n, p.CH);
+    c.a0 = pl.a0;
+    c.b0 = pl.b0;
+    c.cand_cap = pl.cand_cap;
+    c.slot_use = pl.slot_use;
+  }
+  c.IB = index_bits(c.n);
+  c.flip = (p.flags & kFlagLargest) ? KT<VT, SCALE>::KMASK : 0u;
+  c.scaler = 0.f;
+  if constexpr (SCALE) {
+    if (c.n > 0) {
+      float s;
+      if constexpr (VT == kF32) s = __ldg(static_cast<const float*>(p.val_in) + c.in_off);
+      else s = to_float<VT>((uint32_t)__ldg(static_cast<const unsigned short*>(p.val_in) + c.in_off));
+      if (isnan(s) || isinf(s)) s = 0.f;
+      c.scaler = s;
+    }
+  }
+  return c;
+}
+
+// ----------------------------------------------------------------------------
+// Iteration over positions [a, b) of a row.  The unaligned head and tail go
+// through fe(bits, pos, ok) one element per thread; the aligned middle
+// through fv(x, pos0, ok) one 16-byte vector per thread, U vectors in flight.
+// Both callbacks are called by every thread the same number of times (warp
+// collectives are allowed inside).
+// ----------------------------------------------------------------------------
+template <int ES, int U, typename FE, typename FV>
+__device__ __forceinline__ void for_range_v(const void* base, int64_t in_off, int64_t a, int64_t b, FE&& fe,
+                                            FV&& fv) {
+  constexpr int VEC = 16 / ES;
+  if (b <= a) return;
+  const char* row = static_cast<const char*>(base) + in_off * ES;
+  const uintptr_t addr_a = reinterpret_cast<uintptr_t>(row + a * ES);
+  int64_t head = (int64_t)(((16u - (unsigned)(addr_a & 15u)) & 15u) / ES);
+  if (head > b - a) head = b - a;
+  const int64_t va = a + head;
+  const int64_t nvec = (b - va) / VEC;
+  const int64_t vb = va + nvec * VEC;
+  const int64_t tail = b - vb;
+  if (head > 0 || tail > 0) {
+    const int t = threadIdx.x;
+    const bool vh = t < head;
+    const bool vt = t < tail;
+    uint32_t bh = 0, bt = 0;
+    if (vh) bh = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[a + t]
+                         : (uint32_t)reinterpret_cast<const unsigned short*>(row)[a + t];
+    if (vt) bt = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[vb + t]
+                         : (uint32_t)reinterpret_cast<const unsigned short*>(row)[vb + t];
+    if (head > 0) fe(bh, a + t, vh);
+    if (tail > 0) fe(bt, vb + t, vt);
+  }
+  const uint4* vp = reinterpret_cast<const uint4*>(row + va * ES);
+  const int64_t step = (int64_t)kThreads * U;
+  const int64_t iters = (nvec + step - 1) / step;
+  int64_t v0 = threadIdx.x;
+  for (int64_t it = 0; it < iters; ++it, v0 += step) {
+    uint4 x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t v = v0 + (int64_t)u * kThreads;
+      x[u] = v < nvec ? ld_stream16(vp + v) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t v = v0 + (int64_t)u * kThreads;
+      fv(x[u], va + v * VEC, v < nvec);
+    }
+  }
+}
+
+// Element e of a 16-byte vector as a raw bit pattern.
+template <int ES>
+__device__ __forceinline__ uint32_t vec_elem(const uint4& x, int e) {
+  if constexpr (ES == 4) {
+    return e == 0 ? x.x : e == 1 ? x.y : e == 2 ? x.z : x.w;
+  } else {
+    const uint32_t w = (e >> 1) == 0 ? x.x : (e >> 1) == 1 ? x.y : (e >> 1) == 2 ? x.z : x.w;
+    return (e & 1) ? (w >> 16) : (w & 0xFFFFu);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Output writes and warp-staged sinks
+// ----------------------------------------------------------------------------
+template <int VT>
+__device__ __forceinline__ void write_out(const EngineParams& p, int64_t slot, uint32_t bits, int64_t pos) {
+  if constexpr (VT == kF32) static_cast<uint32_t*>(p.val_out)[slot] = bits;
+  else static_cast<unsigned short*>(p.val_out)[slot] = (unsigned short)bits;
+  if (p.flags & kFlagIdx64) static_cast<int64_t*>(p.idx_out)[slot] = pos;
+  else static_cast<int32_t*>(p.idx_out)[slot] = (int32_t)pos;
+}
+
+// Warp-level reservation: every lane passes its count; returns the lane's
+// first slot (base + exclusive prefix).  ctr may be global or shared.
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t cnt, uint32_t* ctr) {
+  const int lane = threadIdx.x & 31;
+  uint32_t x = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  const uint32_t tot = __shfl_sync(kFull, x, 31);
+  uint32_t base = 0;
+  if (tot) {
+    if (lane == 31) base = atomicAdd(ctr, tot);
+    base = __shfl_sync(kFull, base, 31);
+  }
+  return base + x - cnt;
+}
+
+__device__ __forceinline__ uint64_t make_entry(uint32_t bits, int64_t pos) {
+  return ((uint64_t)bits << 32) | (uint64_t)(uint32_t)pos;
+}
+
+// A warp's private staging buffer in shared memory.  Hits are appended with
+// a ballot (no atomics); a full buffer is flushed with one global atomic.
+struct WarpBuf {
+  uint64_t* buf;
+  uint32_t n;  // warp-uniform
+};
+
+template <typename Flush>
+__device__ __forceinline__ void sink_push(WarpBuf& s, int cap, bool want, uint64_t e, Flush&& flush) {
+  const unsigned b = __ballot_sync(kFull, want);
+  if (b == 0) return;
+  const unsigned lane = threadIdx.x & 31u;
+  if (want) s.buf[s.n + __popc(b & ((1u << lane) - 1u))] = e;
+  s.n += (uint32_t)__popc(b);
+  if (s.n > (uint32_t)(cap - 32)) {
+    __syncwarp();
+    flush(s);
+    s.n = 0;
+    __syncwarp();
+  }
+}
+
+// Flushes a warp buffer to the row's output slots.
+template <int VT>
+__device__ __forceinline__ void flush_out(const EngineParams& p, const WarpBuf& s, uint32_t* ctr, int64_t out_off,
+                                          int32_t k) {
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(ctr, s.n);
+  base = __shfl_sync(kFull, base, 0);
+  for (uint32_t i = lane; i < s.n; i += 32) {
+    const uint64_t e = s.buf[i];
+    if (base + i < (uint32_t)k) write_out<VT>(p, out_off + base + i, (uint32_t)(e >> 32), (int64_t)(uint32_t)e);
+  }
+}
+
+// Flushes a warp buffer to a candidate region of capacity cap.
+__device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint64_t* dst, int32_t cap,
+                                           int32_t* status) {
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(ctr, s.n);
+  base = __shfl_sync(kFull, base, 0);
+  for (uint32_t i = lane; i < s.n; i += 32)
+    if (base + i < (uint32_t)cap) dst[base + i] = s.buf[i];
+  (void)status;
+}
+
+// ----------------------------------------------------------------------------
+// Shared-memory selection
+// ----------------------------------------------------------------------------
+// The r-th smallest (1-based) of cnt KB-bit keys in shared memory.
+template <int KB>
+__device__ uint32_t block_kth_key(const uint32_t* keys, int cnt, int r, Misc* m, int32_t* status) {
+  uint32_t prefix = 0;
+  int plen = 0;
+  uint32_t krem = (uint32_t)r;
+  while (plen < KB) {
+    const int D = min(8, KB - plen);
+    for (int i = threadIdx.x; i < 256; i += kThreads) m->hist256[i] = 0;
+    __syncthreads();
+    const int sd = KB - plen - D;
+    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+      const uint32_t k = keys[i];
+      const bool match = plen == 0 || (k >> (KB - plen)) == prefix;
+      if (match) atomicAdd(&m->hist256[(k >> sd) & ((1u << D) - 1u)], 1u);
+    }
+    __syncthreads();
+    block_select<false>(m->hist256, 1 << D, krem, m);
+    if (!m->sel_found) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
+      return (uint32_t)(((uint64_t)1 << KB) - 1);
+    }
+    prefix = (prefix << D) | m->sel_bin;
+    plen += D;
+    krem -= m->sel_cum;
+    __syncthreads();
+  }
+  return prefix;
+}
+
+// Entries get(i) -> (bits, pos), all matching (prefix, plen).  Refines the
+// prefix with 8-bit digits over the composite (key << IB | pos) until the
+// matched set size equals krem.  On return the selected entries are those
+// whose composite prefix is <= prefix.
+template <int VT, bool SCALE, typename G>
+__device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix, int& plen, int& krem, int count,
+                             Misc* m, int32_t* status) {
+  using K = KT<VT, SCALE>;
+  const int W = K::KB + rc.IB;
+  while (count != krem) {
+    if (plen >= W || count < krem) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusLevels);
+      break;
+    }
+    const int D = min(8, W - plen);
+    for (int i = threadIdx.x; i < 256; i += kThreads) m->hist256[i] = 0;
+    __syncthreads();
+    const int sh = W - plen;
+    const int sd = W - plen - D;
+    const uint32_t dm = (1u << D) - 1u;
+    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+      uint32_t bits;
+      int64_t pos;
+      get(i, bits, pos);
+      const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
+      if (shr64(c, sh) == prefix) atomicAdd(&m->hist256[(uint32_t)shr64(c, sd) & dm], 1u);
+    }
+    __syncthreads();
+    block_select<false>(m->hist256, 1 << D, (uint32_t)krem, m);
+    if (!m->sel_found) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
+      break;
+    }
+    prefix = (prefix << D) | m->sel_bin;
+    plen += D;
+    krem -= (int)m->sel_cum;
+    count = (int)m->sel_cnt;
+    __syncthreads();
+  }
+}
+
+// Emits the entries selected by (prefix, plen) to the row's output, in entry
+// order, reserving the slots with one atomic on the row's out_count.
+template <int VT, bool SCALE, typename G>
+__device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& rc, uint64_t prefix, int plen,
+                          RowState* rs, Misc* m) {
+  using K = KT<VT, SCALE>;
+  const int W = K::KB + rc.IB;
+  const int sh = W - plen;
+  const int per = (cnt + kThreads - 1) / kThreads;
+  const int lo = min(cnt, (int)threadIdx.x * per);
+  const int hi = min(cnt, lo + per);
+  uint32_t mine = 0;
+  for (int i = lo; i < hi; ++i) {
+    uint32_t bits;
+    int64_t pos;
+    get(i, bits, pos);
+    const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
+    mine += shr64(c, sh) <= prefix;
+  }
+  uint32_t total;
+  const uint32_t ex = block_excl_scan(mine, m->scan, &total);
+  if (threadIdx.x == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
+  __syncthreads();
+  int64_t slot = (int64_t)m->counter + ex;
+  for (int i = lo; i < hi; ++i) {
+    uint32_t bits;
+    int64_t pos;
+    get(i, bits, pos);
+    const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
+    if (shr64(c, sh) <= prefix) {
+      if (slot < rc.k) write_out<VT>(p, rc.out_off + slot, bits, pos);
+      ++slot;
+    }
+  }
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------------
+// Row post-processing: sort, index mapping, idle fill
+// ----------------------------------------------------------------------------
+template <int VT, bool SCALE>
+__device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* smem, Misc* m) {
+  const int64_t kk = min((int64_t)rc.n, (int64_t)rc.k);
+  const bool idx64 = (p.flags & kFlagIdx64) != 0;
+  const bool withidx = (p.flags & kFlagWithIdxIn) != 0;
+  __threadfence();
+  __syncthreads();
+  auto load_pos = [&](int64_t i) -> int64_t {
+    return idx64 ? (int64_t)__ldcg(reinterpret_cast<const long long*>(p.idx_out) + rc.out_off + i)
+                 : (int64_t)__ldcg(static_cast<const int32_t*>(p.idx_out) + rc.out_off + i);
+  };
+  auto load_bits = [&](int64_t i) -> uint32_t {
+    if constexpr (VT == kF32) return __ldcg(static_cast<const uint32_t*>(p.val_out) + rc.out_off + i);
+    else return (uint32_t)__ldcg(static_cast<const unsigned short*>(p.val_out) + rc.out_off + i);
+  };
+  auto map_idx = [&](int64_t pos) -> int64_t {
+    if (!withidx) return pos;
+    return idx64 ? (int64_t)__ldg(static_cast<const long long*>(p.idx_in) + rc.in_off + pos)
+                 : (int64_t)__ldg(static_cast<const int32_t*>(p.idx_in) + rc.in_off + pos);
+  };
+  if ((p.flags & kFlagSorted) && kk > 1) {
+    const bool ascend = (p.flags & kFlagAscend) != 0;
+    if (kk <= kCapSort) {
+      uint64_t* s = reinterpret_cast<uint64_t*>(smem);
+      int np = 2;
+      while (np < kk) np <<= 1;
+      for (int i = threadIdx.x; i < np; i += kThreads) {
+        uint64_t v = ~0ull;
+        if (i < kk) v = ((uint64_t)out_key<VT>(load_bits(i), ascend) << 32) | (uint64_t)(uint32_t)load_pos(i);
+        s[i] = v;
+      }
+      __syncthreads();
+      block_bitonic_sort(s, np);
+      for (int i = threadIdx.x; i < kk; i += kThreads) {
+        const uint64_t v = s[i];
+        const int64_t pos = (int64_t)(uint32_t)v;
+        write_out<VT>(p, rc.out_off + i, out_key_inv<VT>((uint32_t)(v >> 32), ascend), map_idx(pos));
+      }
+    } else if (rc.sort_off >= 0) {
+      // Merge sort through global scratch: runs of kCapSort sorted in smem,
+      // then pairwise merges (each thread merges a contiguous output range
+      // found by a merge-path search).
+      uint64_t* a = p.sort_scratch + rc.sort_off;
+      uint64_t* b = a + kk;
+      uint64_t* s = reinterpret_cast<uint64_t*>(smem);
+      for (int64_t r0 = 0; r0 < kk; r0 += kCapSort) {
+        const int len = (int)min((int64_t)kCapSort, kk - r0);
+        for (int i = threadIdx.x; i < kCapSort; i += kThreads) {
+          uint64_t v = ~0ull;
+          if (i < len)
+            v = ((uint64_t)out_key<VT>(load_bits(r0 + i), ascend) << 32) | (uint64_t)(uint32_t)load_pos(r0 + i);
+          s[i] = v;
+        }
+        __syncthreads();
+        block_bitonic_sort(s, kCapSort);
+        for (int i = threadIdx.x; i < len; i += kThreads) a[r0 + i] = s[i];
+        __syncthreads();
+      }
+      for (int64_t run = kCapSort; run < kk; run <<= 1) {
+        for (int64_t m0 = 0; m0 < kk; m0 += 2 * run) {
+          const int64_t l0 = m0, l1 = min(kk, m0 + run), r1 = min(kk, m0 + 2 * run);
+          const int64_t tot = r1 - l0;
+          const int64_t per = (tot + kThreads - 1) / kThreads;
+          const int64_t d0 = min(tot, (int64_t)threadIdx.x * per), d1 = min(tot, d0 + per);
+          auto split = [&](int64_t d) -> int64_t {  // elements taken from the left run
+            int64_t lo = max((int64_t)0, d - (r1 - l1)), hi = min(d, l1 - l0);
+            while (lo < hi) {
+              const int64_t mid = (lo + hi) >> 1;
+              if (ld_cg_u64(a + l0 + mid) <= ld_cg_u64(a + l1 + (d - mid - 1))) lo = mid + 1;
+              else hi = mid;
+            }
+            return lo;
+          };
+          if (d0 < d1) {
+            int64_t i = l0 + split(d0), j = l1 + (d0 - (i - l0));
+            for (int64_t d = d0; d < d1; ++d) {
+              const uint64_t x = i < l1 ? ld_cg_u64(a + i) : ~0ull;
+              const uint64_t y = j < r1 ? ld_cg_u64(a + j) : ~0ull;
+              const bool takel = (j >= r1) || (i < l1 && x <= y);
+              b[l0 + d] = takel ? x : y;
+              if (takel) ++i;
+              else ++j;
+            }
+          }
+        }
+        __syncthreads();
+        uint64_t* t = a;
+        a = b;
+        b = t;
+      }
+      for (int64_t i = threadIdx.x; i < kk; i += kThreads) {
+        const uint64_t v = ld_cg_u64(a + i);
+        write_out<VT>(p, rc.out_off + i, out_key_inv<VT>((uint32_t)(v >> 32), ascend), map_idx((int64_t)(uint32_t)v));
+      }
+    }
+  } else if (withidx) {
+    for (int64_t i = threadIdx.x; i < kk; i += kThreads) {
+      const int64_t pos = load_pos(i);
+      const int64_t mapped = map_idx(pos);
+      if (idx64) static_cast<int64_t*>(p.idx_out)[rc.out_off + i] = mapped;
+      else static_cast<int32_t*>(p.idx_out)[rc.out_off + i] = (int32_t)mapped;
+    }
+  }
+  for (int64_t i = kk + threadIdx.x; i < rc.k; i += kThreads) write_out<VT>(p, rc.out_off + i, 0u, -1);
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------------
+// Grid barrier (cooperative launch: all CTAs are resident).  Bounded.
+// ----------------------------------------------------------------------------
+__device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t gen = ld_acquire(&h->bar_gen);
+    __threadfence();
+    const uint32_t arrived = atomicAdd(&h->bar_count, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(&h->bar_count, 0u);
+      __threadfence();
+      st_release(&h->bar_gen, gen + 1u);
+    } else {
+      uint32_t it = 0;
+      while (ld_acquire(&h->bar_gen) == gen) {
+        if (++it > spin_limit) {
+          atomicOr(&h->status, kStatusTimeout);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------------
+// Items
+// ----------------------------------------------------------------------------
+template <int VT, bool SCALE>
+struct Engine {
+  using K = KT<VT, SCALE>;
+  static constexpr int ES = K::ES;
+  static constexpr int VEC = K::VEC;
+  static constexpr int U = 4;
+  static constexpr int kSinkCand = 256;  // candidate entries per warp buffer
+  static constexpr int kSinkOut = 64;    // output entries per warp buffer
+
+  const EngineParams& p;
+  uint8_t* smem;
+  Misc* m;
+
+  __device__ Engine(const EngineParams& p_, uint8_t* s) : p(p_), smem(s), m(misc_of(s)) {}
+
+  __device__ bool spin_until_ge(const uint32_t* addr, uint32_t target) {
+    for (uint32_t it = 0; it < p.spin_limit; ++it) {
+      if (ld_acquire(addr) >= target) return true;
+      __nanosleep(64);
+    }
+    atomicOr(&p.hdr->status, kStatusTimeout);
+    return false;
+  }
+
+  __device__ uint32_t key_of(uint32_t bits, const RowCtx& rc) const {
+    return sel_key<VT, SCALE>(bits, rc.flip, rc.scaler);
+  }
+
+  __device__ uint32_t load_bits(const RowCtx& rc, int64_t pos) const {
+    if constexpr (ES == 4) return __ldg(static_cast<const uint32_t*>(p.val_in) + rc.in_off + pos);
+    else return (uint32_t)__ldg(static_cast<const unsigned short*>(p.val_in) + rc.in_off + pos);
+  }
+
+  // ---- threshold from a strided sample of the row (one CTA).
+  // The sample is S keys in sectors of 32 bytes spread evenly over the row.
+  __device__ uint32_t sample_threshold(const RowCtx& rc) {
+    uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
+    const int S = sample_size(rc.n);
+    constexpr int SE = 32 / ES;  // elements per sector
+    const int nsec = S / SE;
+    const int64_t span = (int64_t)rc.n - SE;
+    for (int j = threadIdx.x; j < S; j += kThreads) {
+      const int i = j / SE, o = j % SE;
+      const int64_t pos = (nsec > 1 ? (int64_t)i * span / (nsec - 1) : 0) + o;
+      keys[j] = key_of(load_bits(rc, pos), rc);
+    }
+    __syncthreads();
+    const uint32_t t = block_kth_key<K::KB>(keys, S, sample_rank(rc.n, rc.k, S), m, &p.hdr->status);
+    __syncthreads();
+    return t;
+  }
+
+  // ---- whole row in shared memory (n <= kSmemRowCap)
+  __device__ void smem_row(int r, const RowCtx& rc) {
+    uint32_t* vals = reinterpret_cast<uint32_t*>(smem);
+    for_range_v<ES, U>(
+        p.val_in, rc.in_off, 0, rc.n, [&](uint32_t bits, int64_t pos, bool ok) { if (ok) vals[pos] = bits; },
+        [&](const uint4& x, int64_t pos0, bool ok) {
+          if (ok) {
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) vals[pos0 + e] = vec_elem<ES>(x, e);
+          }
+        });
+    __syncthreads();
+    const int kk = min(rc.n, rc.k);
+    uint64_t prefix = 0;
+    int plen = 0, krem = kk;
+    auto get = [&](int i, uint32_t& bits, int64_t& pos) {
+      bits = vals[i];
+      pos = i;
+    };
+    smem_resolve<VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, m, &p.hdr->status);
+    smem_emit<VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m);
+    post_process<VT, SCALE>(p, rc, smem + 65536, m);
+  }
+
+  // ---- one CTA, the whole row from global memory (n <= kCtaRowCap)
+  // Pass over the row classifying by a composite prefix; to_out hits go to
+  // the output, to_ent hits into the smem entry array (cap kCapSB).
+  __device__ void cta_filter(const RowCtx& rc, RowState* rs, uint64_t prefix, int plen, bool final_mode,
+                             uint64_t* ent) {
+    const int W = K::KB + rc.IB;
+    const int sh = W - plen;
+    uint32_t* out_ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
+    auto one = [&](uint32_t bits, int64_t pos, bool ok) {
+      bool to_out = false, to_ent = false;
+      if (ok) {
+        const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+        const uint64_t t = shr64(c, sh);
+        to_out = t < prefix || (final_mode && t == prefix);
+        to_ent = !final_mode && t == prefix;
+      }
+      if (!__any_sync(kFull, to_out || to_ent)) return;
+      const uint32_t so = warp_reserve(to_out ? 1u : 0u, out_ctr);
+      if (to_out && so < (uint32_t)rc.k) write_out<VT>(p, rc.out_off + so, bits, pos);
+      const uint32_t se = warp_reserve(to_ent ? 1u : 0u, &m->counter);
+      if (to_ent && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
+    };
+    for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
+    });
+  }
+
+  __device__ void cta_row(int r, const RowCtx& rc) {
+    RowState* rs = p.rs + r;
+    uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
+    auto get = [&](int i, uint32_t& bits, int64_t& pos) {
+      const uint64_t e = ent[i];
+      bits = (uint32_t)(e >> 32);
+      pos = (int64_t)(uint32_t)e;
+    };
+    if ((int64_t)rc.k * kPrefRatio <= rc.n) {
+      // pre-filter inside the CTA
+      const uint32_t T = sample_threshold(rc);
+      if (threadIdx.x == 0) m->counter = 0;
+      __syncthreads();
+      auto one = [&](uint32_t bits, int64_t pos, bool ok) {
+        const bool hit = ok && key_of(bits, rc) <= T;
+        if (!__any_sync(kFull, hit)) return;
+        const uint32_t se = warp_reserve(hit ? 1u : 0u, &m->counter);
+        if (hit && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
+      };
+      for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
+      });
+      __syncthreads();
+      const int c = (int)m->counter;
+      __syncthreads();
+      if (c >= rc.k && c <= kCapSB) {
+        uint64_t prefix = 0;
+        int plen = 0, krem = rc.k;
+        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, m, &p.hdr->status);
+        smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        post_process<VT, SCALE>(p, rc, smem, m);
+        return;
+      }
+      // threshold missed: radix levels below
+    }
+    uint64_t prefix = 0;
+    int plen = 0, krem = rc.k, count = rc.n;
+    const int W = K::KB + rc.IB;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
+    for (int guard = 0; guard < 16 && count != krem && count > kCapSB; ++guard) {
+      const int D = min(12, W - plen);
+      const int NB = 1 << D;
+      for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
+      __syncthreads();
+      const int sh = W - plen, sd = W - plen - D;
+      const uint32_t dm = (uint32_t)NB - 1u;
+      auto one = [&](uint32_t bits, int64_t pos, bool ok) {
+        const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+        hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
+      };
+      for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
+      });
+      __syncthreads();
+      block_select<false>(hist, NB, (uint32_t)krem, m);
+      if (!m->sel_found) {
+        if (threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusSelect);
+        return;
+      }
+      prefix = (prefix << D) | m->sel_bin;
+      plen += D;
+      krem -= (int)m->sel_cum;
+      count = (int)m->sel_cnt;
+      __syncthreads();
+    }
+    const bool final_mode = count == krem;
+    if (threadIdx.x == 0) m->counter = 0;
+    __syncthreads();
+    cta_filter(rc, rs, prefix, plen, final_mode, ent);
+    __syncthreads();
+    if (!final_mode) {
+      const int ne = min((int)m->counter, kCapSB);
+      __syncthreads();
+      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+      smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+    }
+    post_process<VT, SCALE>(p, rc, smem, m);
+  }
+
+  // ---- copy chunk ia of a k >= n row (every element is selected)
+  __device__ bool all_item(int r, const RowCtx& rc, int ia) {
+    RowState* rs = p.rs + r;
+    const int warp = threadIdx.x >> 5;
+    WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + warp * kSinkOut, 0};
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
+    auto fl = [&](const WarpBuf& s) { flush_out<VT>(p, s, ctr, rc.out_off, rc.k); };
+    const int64_t a = (int64_t)ia * p.CH, b = min((int64_t)rc.n, a + p.CH);
+    for_range_v<ES, U>(
+        p.val_in, rc.in_off, a, b,
+        [&](uint32_t bits, int64_t pos, bool ok) { sink_push(ob, kSinkOut, ok, make_entry(bits, pos), fl); },
+        [&](const uint4& x, int64_t pos0, bool ok) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) sink_push(ob, kSinkOut, ok, make_entry(vec_elem<ES>(x, e), pos0 + e), fl);
+        });
+    if (ob.n) fl(ob);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
+    __syncthreads();
+    return m->bcast2 != 0;
+  }
+
+  // ---- sample item of a pre-filter row: publish the threshold
+  __device__ void sample_item(int r, const RowCtx& rc) {
+    const uint32_t T = sample_threshold(rc);
+    if (threadIdx.x == 0) {
+      RowState* rs = p.rs + r;
+      rs->thresh = T;
+      __threadfence();
+      st_release(&rs->ready, 1);
+    }
+  }
+
+  // ---- filter item of a pre-filter row: keys <= T into the candidates
+  __device__ bool pf_item(int r, const RowCtx& rc, int ib) {
+    RowState* rs = p.rs + r;
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      if (spin_until_ge(reinterpret_cast<const uint32_t*>(&rs->ready), 1u)) t = __ldcg(&rs->thresh);
+      else t = 0u;  // timed out: keep nothing (the status bit reports it)
+      m->st_prefix = t;
+    }
+    __syncthreads();
+    const uint32_t T = (uint32_t)m->st_prefix;
+    const int warp = threadIdx.x >> 5;
+    WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
+    uint64_t* dst = p.cand + rc.cand_off;
+    auto fl = [&](const WarpBuf& s) { flush_cand(s, ctr, dst, rc.cand_cap, &p.hdr->status); };
+    const int64_t a = (int64_t)ib * p.CH, b = min((int64_t)rc.n, a + p.CH);
+    const uint32_t flip = rc.flip;
+    const float sc = rc.scaler;
+    for_range_v<ES, U>(
+        p.val_in, rc.in_off, a, b,
+        [&](uint32_t bits, int64_t pos, bool ok) {
+          sink_push(cb, kSinkCand, ok && sel_key<VT, SCALE>(bits, flip, sc) <= T, make_entry(bits, pos), fl);
+        },
+        [&](const uint4& x, int64_t pos0, bool ok) {
+          bool hit[VEC];
+          bool any = false;
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            hit[e] = ok && sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) <= T;
+            any |= hit[e];
+          }
+          if (__any_sync(kFull, any)) {
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) sink_push(cb, kSinkCand, hit[e], make_entry(vec_elem<ES>(x, e), pos0 + e), fl);
+          }
+        });
+    if (cb.n) fl(cb);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->fticket, 1) == rc.nb - 1;
+    __syncthreads();
+    return m->bcast2 != 0;
+  }
+
+  // ---- histogram item of a radix row: first digit of chunk ia
+  __device__ void h_item(int r, const RowCtx& rc, int ia) {
+    const int D1 = p.D1;
+    const int NB = 1 << D1;
+    const int s = rc.slot_use % p.S;
+    const uint32_t use = (uint32_t)(rc.slot_use / p.S);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* ghist = p.hist_ring + (size_t)s * ((size_t)1 << kMaxD1);
+    if (threadIdx.x == 0) m->bcast = use == 0 ? 1 : (int)spin_until_ge(p.slot_gen + s, use);
+    for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) *reinterpret_cast<uint4*>(hist + i) = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    const bool slot_ok = m->bcast != 0;
+    const int shift = K::KB - D1;
+    const int64_t a = (int64_t)ia * p.CH, b = min((int64_t)rc.n, a + p.CH);
+    const uint32_t flip = rc.flip;
+    const float sc = rc.scaler;
+    bool agg = false;
+    for_range_v<ES, U>(
+        p.val_in, rc.in_off, a, b,
+        [&](uint32_t bits, int64_t, bool ok) { hist_add_agg(hist, sel_key<VT, SCALE>(bits, flip, sc) >> shift, ok); },
+        [&](const uint4& x, int64_t, bool ok) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) hist_add(hist, sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) >> shift, ok, e, agg);
+        });
+    __syncthreads();
+    if (slot_ok) {
+      for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) {
+        const uint4 v = *reinterpret_cast<const uint4*>(hist + i);
+        if (v.x) atomicAdd(ghist + i + 0, v.x);
+        if (v.y) atomicAdd(ghist + i + 1, v.y);
+        if (v.z) atomicAdd(ghist + i + 2, v.z);
+        if (v.w) atomicAdd(ghist + i + 3, v.w);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    RowState* rs = p.rs + r;
+    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
+    __syncthreads();
+    if (!m->bcast2) return;
+    // Last histogram item of the row: select the first digit's bin.
+    __threadfence();
+    block_select<true>(ghist, NB, (uint32_t)rc.k, m);
+    const bool found = m->sel_found != 0;
+    const uint32_t bin = m->sel_bin, cum = m->sel_cum, cnt = m->sel_cnt;
+    for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) *reinterpret_cast<uint4*>(ghist + i) = make_uint4(0, 0, 0, 0);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int mode;
+      const int krem = rc.k - (int)cum;
+      if (!found || !slot_ok) {
+        mode = kModeNone;
+        if (!found) atomicOr(&p.hdr->status, kStatusSelect);
+      } else if ((int)cnt == krem) {
+        mode = kModeFinal;
+      } else if ((int)cnt <= kCapSB) {
+        mode = kModeSB;
+      } else if ((int)cnt <= rc.cand_cap) {
+        mode = kModeCand;
+      } else {
+        mode = kModeDefer;
+      }
+      rs->mode = mode;
+      rs->krem = krem;
+      rs->count = (int)cnt;
+      rs->prefix = bin;
+      rs->plen = D1;
+      __threadfence();
+      st_release(p.slot_gen + s, use + 1);
+      st_release(&rs->ready, 1);
+    }
+  }
+
+  // ---- filter item of a radix row
+  __device__ bool f_item(int r, const RowCtx& rc, int ib) {
+    RowState* rs = p.rs + r;
+    if (threadIdx.x == 0) {
+      int mode = kModeNone;
+      if (spin_until_ge(reinterpret_cast<const uint32_t*>(&rs->ready), 1u)) mode = __ldcg(&rs->mode);
+      m->st_mode = mode;
+      m->st_prefix = ld_cg_u64(&rs->prefix);
+    }
+    __syncthreads();
+    const int mode = m->st_mode;
+    if (mode == kModeFinal || mode == kModeSB || mode == kModeCand) {
+      const uint32_t prefix = (uint32_t)m->st_prefix;
+      const int shift = K::KB - p.D1;
+      const bool final_mode = mode == kModeFinal;
+      const int warp = threadIdx.x >> 5;
+      WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
+      WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + kWarps * kSinkCand + warp * kSinkOut, 0};
+      uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
+      uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
+      uint64_t* dst = p.cand + rc.cand_off;
+      auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, rc.cand_cap, &p.hdr->status); };
+      auto flo = [&](const WarpBuf& s) { flush_out<VT>(p, s, octr, rc.out_off, rc.k); };
+      const uint32_t flip = rc.flip;
+      const float sc = rc.scaler;
+      auto one = [&](uint32_t bits, int64_t pos, bool ok) {
+        const uint32_t d = sel_key<VT, SCALE>(bits, flip, sc) >> shift;
+        const bool to_out = ok && (d < prefix || (final_mode && d == prefix));
+        const bool to_cand = ok && !final_mode && d == prefix;
+        sink_push(ob, kSinkOut, to_out, make_entry(bits, pos), flo);
+        sink_push(cb, kSinkCand, to_cand, make_entry(bits, pos), flc);
+      };
+      const int64_t a = (int64_t)ib * p.CH, b = min((int64_t)rc.n, a + p.CH);
+      for_range_v<ES, U>(p.val_in, rc.in_off, a, b, one, [&](const uint4& x, int64_t pos0, bool ok) {
+        bool any = false;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) any |= ok && (sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) >> shift) <= prefix;
+        if (__any_sync(kFull, any)) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
+        }
+      });
+      if (ob.n) flo(ob);
+      if (cb.n) flc(cb);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->fticket, 1) == rc.nb - 1;
+    __syncthreads();
+    return m->bcast2 != 0;
+  }
+
+  // Hands a row to phase B.
+  __device__ void to_phase_b(int r, int src, int src_len, uint64_t prefix, int plen, int krem, int count) {
+    if (threadIdx.x == 0) {
+      RowState* rs = p.rs + r;
+      rs->src = src;
+      rs->src_len = src_len;
+      rs->prefix = prefix;
+      rs->plen = plen;
+      rs->krem = krem;
+      rs->count = count;
+      rs->final_pass = 0;
+      rs->sb_count = 0;
+      __threadfence();
+      const int slot = atomicAdd(&p.hdr->nlarge, 1);
+      p.large_list[slot] = r;
+    }
+  }
+
+  // Finisher work of a large row (all of its items are done).
+  __device__ void finish_row(int r) {
+    const RowCtx rc = load_row<VT, SCALE>(p, r);
+    RowState* rs = p.rs + r;
+    __threadfence();
+    if (threadIdx.x == 0) {
+      m->st_mode = rc.kind == kKindAll ? kModeAll : __ldcg(&rs->mode);
+      m->st_krem = __ldcg(&rs->krem);
+      m->st_count = __ldcg(&rs->count);
+      m->st_plen = __ldcg(&rs->plen);
+      m->st_prefix = ld_cg_u64(&rs->prefix);
+      m->st_candn = __ldcg(&rs->cand_count);
+    }
+    __syncthreads();
+    uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
+    auto get = [&](int i, uint32_t& bits, int64_t& pos) {
+      const uint64_t e = ent[i];
+      bits = (uint32_t)(e >> 32);
+      pos = (int64_t)(uint32_t)e;
+    };
+    const uint64_t* cand = p.cand + rc.cand_off;
+    if (rc.kind == kKindGridPref) {
+      const int c = m->st_candn;
+      if (c >= rc.k && c <= kCapSB) {
+        for (int i = threadIdx.x; i < c; i += kThreads) ent[i] = ld_cg_u64(cand + i);
+        __syncthreads();
+        uint64_t prefix = 0;
+        int plen = 0, krem = rc.k;
+        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, m, &p.hdr->status);
+        smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        post_process<VT, SCALE>(p, rc, smem, m);
+      } else if (c >= rc.k && c <= rc.cand_cap) {
+        to_phase_b(r, 1, c, 0, 0, rc.k, c);
+      } else {
+        to_phase_b(r, 0, rc.n, 0, 0, rc.k, rc.n);
+      }
+      return;
+    }
+    const int mode = m->st_mode;
+    if (mode == kModeSB) {
+      const int ne = min(m->st_candn, kCapSB);
+      for (int i = threadIdx.x; i < ne; i += kThreads) ent[i] = ld_cg_u64(cand + i);
+      uint64_t prefix = m->st_prefix;
+      int plen = m->st_plen, krem = m->st_krem;
+      __syncthreads();
+      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+      smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      post_process<VT, SCALE>(p, rc, smem, m);
+    } else if (mode == kModeCand) {
+      to_phase_b(r, 1, min(m->st_candn, rc.cand_cap), m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+    } else if (mode == kModeDefer) {
+      to_phase_b(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+    } else if (mode == kModeFinal || mode == kModeAll) {
+      post_process<VT, SCALE>(p, rc, smem, m);
+    }
+  }
+
+  // ---- phase B: multi-CTA radix levels over the listed rows ----
+  struct PBTable {
+    int32_t row[kPhaseBSlots];
+    int32_t nch[kPhaseBSlots];
+    int32_t c0[kPhaseBSlots + 1];
+  };
+
+  // Runs f(bits, pos, ok) over entries [a, b) of a phase-B source.
+  template <typename Fn>
+  __device__ void pb_source(const RowCtx& rc, int src, int64_t a, int64_t b, Fn&& fn) {
+    if (src == 1) {
+      const uint64_t* cand = p.cand + rc.cand_off;
+      const int64_t cnt = b - a;
+      const int64_t iters = (cnt + kThreads - 1) / kThreads;
+      for (int64_t it = 0; it < iters; ++it) {
+        const int64_t i = a + it * kThreads + threadIdx.x;
+        const bool ok = i < b;
+        const uint64_t e = ok ? ld_cg_u64(cand + i) : 0ull;
+        fn((uint32_t)(e >> 32), (int64_t)(uint32_t)e, ok);
+      }
+    } else {
+      for_range_v<ES, U>(p.val_in, rc.in_off, a, b, fn, [&](const uint4& x, int64_t pos0, bool ok) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) fn(vec_elem<ES>(x, e), pos0 + e, ok);
+      });
+    }
+  }
+
+  // Builds the table of the first nG listed rows whose flag matches `want`
+  // (0: rows that still need a histogram level, 1: rows due for the final
+  // filter).  Returns the number of chunks.
+  __device__ int pb_table(PBTable* t, int nG, int want) {
+    if (threadIdx.x == 0) {
+      int c = 0;
+      for (int i = 0; i < nG; ++i) {
+        const int r = p.large_list[i];
+        const RowState* rs = p.rs + r;
+        const int fp = __ldcg(&rs->final_pass);
+        const int len = __ldcg(&rs->src_len);
+        t->row[i] = r;
+        t->c0[i] = c;
+        t->nch[i] = (fp == want) ? (len + kPhaseBChunk - 1) / kPhaseBChunk : 0;
+        c += t->nch[i];
+      }
+      t->c0[nG] = c;
+    }
+    __syncthreads();
+    return t->c0[nG];
+  }
+
+  __device__ void phase_b() {
+    PBTable* t = reinterpret_cast<PBTable*>(m->pbtab);
+    for (int round = 0; round < 64; ++round) {
+      grid_barrier(p.hdr, p.spin_limit);
+      const int nL = __ldcg(&p.hdr->nlarge);
+      if (nL <= 0) return;
+      const int nG = min(nL, kPhaseBSlots);
+      // rows already small enough skip the histogram
+      for (int i = blockIdx.x; i < nG; i += gridDim.x) {
+        if (threadIdx.x == 0) {
+          RowState* rs = p.rs + p.large_list[i];
+          const int cnt = __ldcg(&rs->count), kr = __ldcg(&rs->krem);
+          rs->final_pass = (cnt == kr || cnt <= kCapSB) ? 1 : 0;
+        }
+      }
+      grid_barrier(p.hdr, p.spin_limit);
+      // ---- histogram of the next 12-bit digit
+      int total = pb_table(t, nG, 0);
+      uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
+      for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int i = 0;
+        while (t->c0[i + 1] <= w) ++i;
+        const int r = t->row[i];
+        const RowCtx rc = load_row<VT, SCALE>(p, r);
+        const RowState* rs = p.rs + r;
+        const uint64_t prefix = ld_cg_u64(&rs->prefix);
+        const int plen = __ldcg(&rs->plen);
+        const int src = __ldcg(&rs->src);
+        const int len = __ldcg(&rs->src_len);
+        const int W = K::KB + rc.IB;
+        const int D = min(12, W - plen);
+        const int NB = 1 << D;
+        for (int j = threadIdx.x; j < NB; j += kThreads) hist[j] = 0;
+        __syncthreads();
+        const int sh = W - plen, sd = W - plen - D;
+        const uint32_t dm = (uint32_t)NB - 1u;
+        const int64_t a = (int64_t)(w - t->c0[i]) * kPhaseBChunk, b = min((int64_t)len, a + kPhaseBChunk);
+        pb_source(rc, src, a, b, [&](uint32_t bits, int64_t pos, bool ok) {
+          const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+          hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
+        });
+        __syncthreads();
+        uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
+        for (int j = threadIdx.x; j < NB; j += kThreads)
+          if (hist[j]) atomicAdd(gh + j, hist[j]);
+        __syncthreads();
+      }
+      grid_barrier(p.hdr, p.spin_limit);
+      // ---- bin selection, one CTA per row
+      for (int i = blockIdx.x; i < nG; i += gridDim.x) {
+        const int r = p.large_list[i];
+        RowState* rs = p.rs + r;
+        if (__ldcg(&rs->final_pass)) continue;
+        const RowCtx rc = load_row<VT, SCALE>(p, r);
+        const int plen = __ldcg(&rs->plen);
+        const int W = K::KB + rc.IB;
+        const int D = min(12, W - plen);
+        const int NB = 1 << D;
+        uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
+        const int krem = __ldcg(&rs->krem);
+        block_select<true>(gh, NB, (uint32_t)krem, m);
+        const bool found = m->sel_found != 0;
+        const uint32_t bin = m->sel_bin, cum = m->sel_cum, cnt = m->sel_cnt;
+        for (int j = threadIdx.x; j < NB; j += kThreads) gh[j] = 0;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          if (!found) {
+            atomicOr(&p.hdr->status, kStatusSelect);
+            rs->count = krem;  // give up on this row: finish what is there
+            rs->final_pass = 1;
+          } else {
+            rs->prefix = (ld_cg_u64(&rs->prefix) << D) | bin;
+            rs->plen = plen + D;
+            rs->krem = krem - (int)cum;
+            rs->count = (int)cnt;
+            rs->final_pass = ((int)cnt == krem - (int)cum || (int)cnt <= kCapSB) ? 1 : 0;
+          }
+        }
+        __syncthreads();
+      }
+      grid_barrier(p.hdr, p.spin_limit);
+      // ---- final filter for the rows that are due
+      total = pb_table(t, nG, 1);
+      const int warp = threadIdx.x >> 5;
+      for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int i = 0;
+        while (t->c0[i + 1] <= w) ++i;
+        const int r = t->row[i];
+        const RowCtx rc = load_row<VT, SCALE>(p, r);
+        RowState* rs = p.rs + r;
+        const uint64_t prefix = ld_cg_u64(&rs->prefix);
+        const int plen = __ldcg(&rs->plen);
+        const int src = __ldcg(&rs->src);
+        const int len = __ldcg(&rs->src_len);
+        const bool final_mode = __ldcg(&rs->count) == __ldcg(&rs->krem);
+        const int W = K::KB + rc.IB;
+        const int sh = W - plen;
+        WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
+        WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + kWarps * kSinkCand + warp * kSinkOut, 0};
+        uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->sb_count);
+        uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
+        uint64_t* dst = p.pb_sb + (size_t)i * kCapSB;
+        auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, kCapSB, &p.hdr->status); };
+        auto flo = [&](const WarpBuf& s) { flush_out<VT>(p, s, octr, rc.out_off, rc.k); };
+        const int64_t a = (int64_t)(w - t->c0[i]) * kPhaseBChunk, b = min((int64_t)len, a + kPhaseBChunk);
+        pb_source(rc, src, a, b, [&](uint32_t bits, int64_t pos, bool ok) {
+          const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+          const uint64_t tt = shr64(c, sh);
+          sink_push(ob, kSinkOut, ok && (tt < prefix || (final_mode && tt == prefix)), make_entry(bits, pos), flo);
+          sink_push(cb, kSinkCand, ok && !final_mode && tt == prefix, make_entry(bits, pos), flc);
+        });
+        if (ob.n) flo(ob);
+        if (cb.n) flc(cb);
+        __syncthreads();
+      }
+      grid_barrier(p.hdr, p.spin_limit);
+      // ---- finish the rows that were filtered
+      uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
+      for (int i = blockIdx.x; i < nG; i += gridDim.x) {
+        const int r = p.large_list[i];
+        RowState* rs = p.rs + r;
+        if (!__ldcg(&rs->final_pass)) continue;
+        const RowCtx rc = load_row<VT, SCALE>(p, r);
+        const int count = __ldcg(&rs->count), krem0 = __ldcg(&rs->krem);
+        if (count != krem0) {
+          const int ne = min(__ldcg(&rs->sb_count), kCapSB);
+          const uint64_t* sb = p.pb_sb + (size_t)i * kCapSB;
+          for (int j = threadIdx.x; j < ne; j += kThreads) ent[j] = ld_cg_u64(sb + j);
+          uint64_t prefix = ld_cg_u64(&rs->prefix);
+          int plen = __ldcg(&rs->plen), krem = krem0;
+          __syncthreads();
+          auto get = [&](int j, uint32_t& bits, int64_t& pos) {
+            const uint64_t e = ent[j];
+            bits = (uint32_t)(e >> 32);
+            pos = (int64_t)(uint32_t)e;
+          };
+          smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+          smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+        }
+        post_process<VT, SCALE>(p, rc, smem, m);
+        if (threadIdx.x == 0) rs->final_pass = 2;  // done
+      }
+      grid_barrier(p.hdr, p.spin_limit);
+      // ---- drop the finished rows from the list (CTA 0)
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int w = 0;
+        for (int i = 0; i < nL; ++i) {
+          const int r = p.large_list[i];
+          if (i < nG && __ldcg(&p.rs[r].final_pass) == 2) continue;
+          p.large_list[w++] = r;
+        }
+        p.hdr->nlarge = w;
+        __threadfence();
+      }
+    }
+    if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(&p.hdr->status, kStatusLevels);
+  }
+};
+
+// Maps a claim index to an item.  Returns true for an A item; idx is the
+// item's index in its sequence.
+__device__ __forceinline__ bool decode_item(int q, int NA, int NB, int L, int& idx) {
+  const int L1 = min(L, NA);
+  if (q < L1) {
+    idx = q;
+    return true;
+  }
+  const int q1 = q - L1;
+  const int P = min(NA - L1, NB);
+  if (q1 < 2 * P) {
+    const int mth = q1 >> 1;
+    if ((q1 & 1) == 0) {
+      idx = L1 + mth;
+      return true;
+    }
+    idx = mth;
+    return false;
+  }
+  const int rest = q1 - 2 * P;
+  if (NA - L1 > P) {
+    idx = L1 + P + rest;
+    return true;
+  }
+  idx = P + rest;
+  return false;
+}
+
+template <int VT, bool SCALE>
+__global__ void __launch_bounds__(kThreads, 1) engine_kernel(const __grid_constant__ EngineParams p) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  Engine<VT, SCALE> e(p, smem);
+  Misc* m = e.m;
+  if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
+  int NA, NB, lag;
+  if (p.uniform) {
+    const int kind = row_kind(p.u_n, p.u_k);
+    NA = p.B * row_na(kind, p.u_n, p.CH);
+    NB = p.B * row_nb(kind, p.u_n, p.CH);
+    lag = p.lag;
+  } else {
+    NA = __ldcg(&p.hdr->na);
+    NB = __ldcg(&p.hdr->nb);
+    lag = __ldcg(&p.hdr->lag);
+  }
+  const int NQ = NA + NB;
+  if (threadIdx.x == 0) m->next_q = (int)atomicAdd(&p.hdr->qhead, 1u);
+  __syncthreads();
+  int q = m->next_q;
+  int pending = -1;
+  while (true) {
+    if (q >= NQ) {
+      if (pending >= 0) e.finish_row(pending);
+      break;
+    }
+    __syncthreads();
+    const bool prefetch = pending < 0;
+    uint32_t nq = 0;
+    if (threadIdx.x == 0 && prefetch) nq = atomicAdd(&p.hdr->qhead, 1u);
+    int idx;
+    const bool isA = decode_item(q, NA, NB, lag, idx);
+    int r;
+    if (p.uniform) {
+      const int kind = row_kind(p.u_n, p.u_k);
+      r = isA ? idx / row_na(kind, p.u_n, p.CH) : idx / max(1, row_nb(kind, p.u_n, p.CH));
+    } else {
+      r = isA ? p.a_row[idx] : p.b_row[idx];
+    }
+    const RowCtx rc = load_row<VT, SCALE>(p, r);
+    int fin = -1;
+    if (isA) {
+      switch (rc.kind) {
+        case kKindSmem: e.smem_row(r, rc); break;
+        case kKindCta: e.cta_row(r, rc); break;
+        case kKindAll:
+          if (e.all_item(r, rc, idx - rc.a0)) fin = r;
+          break;
+        case kKindGridPref: e.sample_item(r, rc); break;
+        case kKindGridRadix: e.h_item(r, rc, idx - rc.a0); break;
+        default: break;
+      }
+    } else {
+      if (rc.kind == kKindGridPref) {
+        if (e.pf_item(r, rc, idx - rc.b0)) fin = r;
+      } else if (rc.kind == kKindGridRadix) {
+        if (e.f_item(r, rc, idx - rc.b0)) fin = r;
+      }
+    }
+    if (pending >= 0) {
+      e.finish_row(pending);
+      pending = -1;
+    }
+    pending = fin;
+    __syncthreads();
+    if (threadIdx.x == 0) m->next_q = prefetch ? (int)nq : (int)atomicAdd(&p.hdr->qhead, 1u);
+    __syncthreads();
+    q = m->next_q;
+  }
+  e.phase_b();
+}
+
+}  // namespace dev
+
+template <int VT, bool SCALE>
+inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t stream) {
+  auto kern = dev::engine_kernel<VT, SCALE>;
+  // The smem opt-in is per device; remember which devices have it.
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  // Cooperative launch: phase B synchronises the grid, so every CTA must be
+  // resident (one per SM).
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemBytes;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, p);
+}
+
+// Occupancy of one engine instantiation (CTAs per SM with its smem opt-in).
+template <int VT, bool SCALE>
+inline cudaError_t engine_occupancy(int* per_sm) {
+  const void* fn = (const void*)dev::engine_kernel<VT, SCALE>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, kThreads, kSmemBytes);
+}
+
+// Per value type entry points (one translation unit each).
+cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_engine_bf16(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t occupancy_f32(uint32_t flags, int* per_sm);
+cudaError_t occupancy_f16(uint32_t flags, int* per_sm);
+cudaError_t occupancy_bf16(uint32_t flags, int* per_sm);
+
+}  // namespace radik

@@ -1,0 +1,16 @@
+// radik_engine_f16.cu -- f16 instantiations of the selection engine
+// (split per value type so the three compile in parallel).
+#include "radik_engine.cuh"
+
+namespace radik {
+
+cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream) {
+  return (p.flags & kFlagWithScale) ? launch_typed<kF16, true>(p, grid, stream)
+                                    : launch_typed<kF16, false>(p, grid, stream);
+}
+
+cudaError_t occupancy_f16(uint32_t flags, int* per_sm) {
+  return (flags & kFlagWithScale) ? engine_occupancy<kF16, true>(per_sm) : engine_occupancy<kF16, false>(per_sm);
+}
+
+}  // namespace radik

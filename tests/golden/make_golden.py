@@ -20,6 +20,8 @@ import oracle  # noqa: E402
 from radik_b200 import workloads  # noqa: E402
 
 # name, dtype, lengths, K, largest, ascend, withscale, sorted, distribution, seed
+# (no row shorter than K: the reference launches a zero-sized grid for it and
+# raises "invalid configuration argument", topk_radixselect.h:158-168)
 CASES = [
     ("f32_u01_largest_unsorted", oracle.F32, [3000] * 4, 32, 1, 0, 0, 0, "u01", 1),
     ("f32_u01_largest_sorted_multichunk", oracle.F32, [70000], 256, 1, 0, 0, 1, "u01", 2),
@@ -27,7 +29,6 @@ CASES = [
     ("f16_u01_largest_sorted", oracle.F16, [4000] * 4, 64, 1, 0, 0, 1, "u01", 4),
     ("f32_u0607_scaled_largest_sorted", oracle.F32, [20000] * 2, 1024, 1, 0, 1, 1, "u0607", 5),
     ("f16_u0607_scaled_smallest_unsorted", oracle.F16, [6000] * 2, 77, 0, 1, 1, 0, "u0607", 6),
-    ("f32_short_rows_idle_fill_sorted", oracle.F32, [1000, 700], 1200, 1, 0, 0, 1, "normal", 7),
     ("f32_all_zero_unsorted", oracle.F32, [5000], 50, 1, 0, 0, 0, "zero", 8),
     ("f32_uneven_lengths_sorted", oracle.F32, [7400, 8800, 8000, 7300, 8700], 128, 0, 1, 0, 1, "u01", 9),
     ("f32_u12867_largest_unsorted", oracle.F32, [40000], 500, 1, 0, 0, 0, "u128", 10),

@@ -69,7 +69,9 @@ SHAPES = [
     (1, 1 << 20, 256),      # single-row benchmark shape
     (8, 1 << 20, 1024),
     (4, 300000, 4096),
-    (2, 50000, 20000),      # k > sort cap (merge sort path when sorted)
+    (2, 50000, 20000),      # one-CTA row, k > sort cap (merge sort path when sorted)
+    (2, 1 << 20, 20000),    # radix grid rows (k * 64 > n)
+    (3, 300000, 6000),      # radix grid rows just above the one-CTA cap
 ]
 
 
@@ -84,7 +86,7 @@ def test_parity_vs_oracle(shape, dtype, largest, sorted_):
 
 
 @pytest.mark.parametrize("dist", ["u01", "ties", "zero", "mantissa_noise", "constant_heavy", "zipf"])
-@pytest.mark.parametrize("n,k", [(70000, 100), (1 << 20, 2048), (20000, 5000)])
+@pytest.mark.parametrize("n,k", [(70000, 100), (1 << 20, 2048), (20000, 5000), (1 << 20, 20000)])
 def test_parity_distributions(dist, n, k):
     flat = values_for(rk.F32, n, dist, 5)
     for largest in (True, False):
@@ -206,3 +208,22 @@ def test_value_multisets_match_reference_radik(ref, case):
         if sorted_:
             assert np.array_equal(rv[r], ov[r]), f"row {r} sorted sequence"
         assert np.array_equal(rows[r][ri[r]], rv[r]) and len(np.unique(ri[r])) == k
+
+
+@pytest.mark.parametrize("dist", ["mantissa_noise", "zipf", "constant_heavy", "zero"])
+def test_phase_b_large_rows(dist):
+    """Rows whose threshold misses or whose selected bin is huge finish in the
+    multi-CTA levels; results must still be exact."""
+    n = 1 << 22
+    flat = values_for(rk.F32, n, dist, 77)
+    for largest, k in ((False, 4096), (True, 100000), (True, 64)):
+        got, want = run_both(flat, [n], k, rk.F32, largest, False)
+        assert_same_selection(got, want, [n], [k], [0], False, f"{dist} largest={largest} k={k}")
+
+
+def test_status_is_clean_after_calls():
+    n = 1 << 20
+    t = to_dev(values_for(rk.F32, 2 * n, "u01", 3), rk.F32)
+    ws = torch.empty(rk.get_radix_select_l_workspace_size(rk.F32, 256, n, 2), dtype=torch.uint8, device=DEV)
+    rk.topk(t, 256, [n, n], workspace=ws, check=False)
+    assert rk.status(ws) == 0

@@ -19,7 +19,7 @@
 namespace radik {
 
 cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
-cudaError_t launch_plan(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* a_row,
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
                         int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
                         int64_t sort_cap_total, int grid, cudaStream_t stream);
 cudaError_t engine_max_grid(int dtype, uint32_t flags, int* grid);
@@ -29,7 +29,7 @@ namespace {
 constexpr uint32_t kKnownFlags = kFlagLargest | kFlagSorted | kFlagAscend | kFlagWithScale | kFlagWithIdxIn | kFlagIdx64;
 constexpr int kSlots = 64;             // level-1 histogram ring slots
 constexpr int kMinCH = 4096;           // chunk length bounds (elements)
-constexpr int kMaxCH = 65536;
+constexpr int kMaxCH = 1 << 18;
 constexpr uint32_t kSpinLimit = 1u << 23;
 
 thread_local std::string g_last_error;
@@ -106,7 +106,7 @@ Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
   Bounds b{};
   const int64_t nch = std::max<int64_t>(1, ceil_div(n_max, kMinCH));
   b.na = B * nch;
-  b.nb = B * nch;
+  b.nb = B * (nch + 1);
   b.cand = n_max > kCtaRowCap ? B * (int64_t)cand_capacity((int32_t)n_max) : 0;
   const int64_t kk = std::min(n_max, K);
   b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? B * 2 * kk : 0;
@@ -116,7 +116,7 @@ Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
 Bounds bounds_rows(int64_t B, int64_t total_n, int64_t n_max, int64_t k_max, uint32_t flags) {
   Bounds b{};
   b.na = total_n / kMinCH + B;
-  b.nb = total_n / kMinCH + B;
+  b.nb = total_n / kMinCH + 2 * B;
   b.cand = std::min(total_n, B * (int64_t)kCapSB) + total_n / 8 + B;
   const int64_t kk = std::min(n_max, k_max);
   b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * std::min(total_n, B * k_max) : 0;
@@ -129,25 +129,30 @@ int env_int(const char* name, int dflt) {
   return std::atoi(v);
 }
 
-// Tunables: chunk length and first-digit width.  The defaults aim at about
-// four chunks per CTA so the work queue balances, with chunks of 4K..64K
-// elements, and a 14-bit first digit (16384 bins, 64 KB of shared memory):
-// for i.i.d. fp32 rows the selected bin then holds about n/64 keys, which a
-// finisher resolves in shared memory.  RADIK_CH / RADIK_D1 override them
-// (tuning sweeps).
+// Tunables: chunk lengths and first-digit width.  Single-read rows use
+// chunks of 4K..256K elements, aiming at about four chunks per CTA so the
+// work queue balances while each chunk streams long enough to amortise its
+// item overhead.  Radix rows use 32K-element chunks: their filter items
+// re-read chunks that the histogram items read two grids earlier, and that
+// window (2 x 148 x 128 KB) must stay in L2.  The 14-bit first digit (16384
+// bins, 64 KB of smem) leaves about n/64 keys of an i.i.d. fp32 row in the
+// selected bin.  RADIK_CH / RADIK_CHR / RADIK_D1 override (tuning sweeps).
 struct Config {
-  int CH, D1;
+  int CH, CHR, D1;
 };
 
-Config choose_config(int64_t multi_elems, int grid) {
+Config choose_config(int64_t stream_elems, int grid) {
   Config c{};
-  const int64_t target = std::max<int64_t>(1, multi_elems / ((int64_t)grid * 4));
+  const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 4));
   int ch = kMinCH;
   while (ch < kMaxCH && ch * 2 <= target) ch *= 2;
   c.CH = ch;
+  c.CHR = 32768;
   c.D1 = kMaxD1;
   const int ech = env_int("RADIK_CH", 0);
   if (ech >= kMinCH && ech <= (1 << 24) && (ech % 16) == 0) c.CH = ech;
+  const int echr = env_int("RADIK_CHR", 0);
+  if (echr >= kMinCH && echr <= (1 << 24) && (echr % 16) == 0) c.CHR = echr;
   const int ed1 = env_int("RADIK_D1", 0);
   if (ed1 >= kMinD1 && ed1 <= kMaxD1) c.D1 = ed1;
   return c;
@@ -184,6 +189,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.pb_sb = reinterpret_cast<uint64_t*>(ws + L.pb_sb);
   p.B = B;
   p.CH = c.CH;
+  p.CHR = c.CHR;
   p.D1 = c.D1;
   p.S = kSlots;
   p.flags = flags;
@@ -191,13 +197,22 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   return p;
 }
 
-size_t zero_bytes(const Layout& L) { return L.zero_end; }
+// Bytes cleared before a call: the header, row states and ring release
+// counters always; the histogram ring only when radix rows may use it in
+// phase A (phase B clears the slots it uses).
+size_t zero_bytes(const Layout& L, bool with_hist) { return with_hist ? L.zero_end : L.hist; }
 
 // How far A items run ahead of B items beyond what correctness needs.
 // Radix rows re-read their chunks in B items, so their A items run two grids
 // ahead and the re-reads hit L2; pre-filter rows read their chunks once and
 // only need their sample item done, so a short lead suffices.
 int64_t lag_floor(bool has_radix, int grid) { return has_radix ? 2 * (int64_t)grid : std::max(2, grid / 4); }
+
+// Rows a FIN item trails its row in the B sequence: about one and a half
+// grids of chunk items for uniform rows (their chunks are done by then); a
+// fixed 64 rows for planned batches.
+constexpr int kFinDelayRows = 64;
+int fin_delay_uniform(int nc, int grid) { return std::max(1, (3 * grid + 2 * std::max(nc, 1) - 1) / (2 * std::max(nc, 1))); }
 
 }  // namespace
 }  // namespace radik
@@ -266,16 +281,14 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
   if (rc) return rc;
   const Config cfg = choose_config(multi_elems, grid);
   // exact needs of this call
-  int64_t na = 0, nb = 0, cand = 0, sortn = 0, maxlag = 0;
+  int64_t na = 0, nb = 0, cand = 0, sortn = 0;
   bool has_radix = false;
   for (int i = 0; i < B; ++i) {
     const int n = task_len[i];
     const int kind = row_kind(n, K);
     has_radix = has_radix || kind == kKindGridRadix;
-    const int64_t ra = row_na(kind, n, cfg.CH), rb = row_nb(kind, n, cfg.CH);
-    if (rb > 0) maxlag = std::max(maxlag, na + ra - nb);
-    na += ra;
-    nb += rb;
+    na += row_na(kind, n, cfg.CH, cfg.CHR);
+    nb += row_nbc(kind, n, cfg.CH, cfg.CHR) + row_fin(kind);
     cand += row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     if ((flags & kFlagSorted) && kk > kCapSort) sortn += 2 * kk;
@@ -284,7 +297,7 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
   const Layout L = make_layout(B, na, nb, cand, sortn);
   if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
   uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L), stream);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, has_radix), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
   if (uniform) {
@@ -296,6 +309,20 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
     p.u_cand_cap = row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
+    // B sequence layout (see uniform_b_item) and the lag it needs
+    const int64_t una = row_na(kind, n, cfg.CH, cfg.CHR), nc = row_nbc(kind, n, cfg.CH, cfg.CHR);
+    const int64_t f = row_fin(kind);
+    const int D = fin_delay_uniform((int)nc, grid);
+    const int64_t Dd = std::min<int64_t>(D, B);
+    auto b0 = [&](int64_t q) { return q < Dd ? q * nc : Dd * nc + (q - Dd) * (nc + f); };
+    int64_t maxlag = 0;
+    for (int64_t r = 0; r < B && (nc > 0 || f); ++r) {
+      int64_t first_b;
+      if (nc > 0) first_b = b0(r);
+      else first_b = (r + Dd < B) ? b0(r + Dd) + nc : (int64_t)B * nc + f * (B - Dd) + (r - (B - Dd));
+      maxlag = std::max(maxlag, (r + 1) * una - first_b);
+    }
+    p.fin_delay = D;
     p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(has_radix, grid));
   } else {
     std::vector<RowDesc> d(B);
@@ -313,7 +340,7 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
     p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
     p.a_row = reinterpret_cast<int32_t*>(ws + L.a_row);
     p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
-    e = launch_plan(dd, B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans), reinterpret_cast<int32_t*>(ws + L.a_row),
+    e = launch_plan(dd, B, cfg.CH, cfg.CHR, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans), reinterpret_cast<int32_t*>(ws + L.a_row),
                     reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, na, nb, cand, sortn, grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "plan launch");
   }
@@ -342,7 +369,7 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   if (rc) return rc;
   const Config cfg = choose_config(total_n, grid);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L), stream);
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, true), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
   p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
@@ -350,7 +377,7 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
   // The item budget assumed kMinCH-long chunks; with the chosen CH the true
   // count is smaller, so the bound still holds.
-  e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
+  e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, cfg.CHR, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
                   reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, b.na, b.nb,
                   b.cand, b.sort, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan launch");

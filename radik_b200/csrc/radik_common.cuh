@@ -33,20 +33,21 @@ enum : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 // ----------------------------------------------------------------------------
 // Engine geometry
 // ----------------------------------------------------------------------------
-constexpr int kThreads = 1024;           // one CTA per SM, 32 warps
+constexpr int kThreads = 512;            // two CTAs per SM, 16 warps each
+constexpr int kCtasPerSM = 2;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCapSB = 24576;            // candidates a finisher resolves in smem
-constexpr int kSmemRowCap = 16384;       // rows this short are selected in smem
+constexpr int kCapSB = 10240;            // candidates a finisher resolves in smem (80 KB)
+constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
 constexpr int kCtaRowCap = 1 << 18;      // rows this short are selected by one CTA
-constexpr int kCapSort = 16384;          // outputs a finisher sorts in smem
-constexpr int kMaxD1 = 14;               // widest first digit (64 KB smem hist)
+constexpr int kCapSort = 8192;           // outputs a finisher sorts in smem (64 KB)
+constexpr int kMaxD1 = 12;               // widest first digit (16 KB smem hist)
 constexpr int kMinD1 = 8;
 constexpr int kPrefRatio = 64;           // pre-filter rows with k * 64 <= n
 constexpr int kSampleMax = 16384;        // sampled keys per row (64 KB smem)
 constexpr int kSampleMin = 1024;
 constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
 constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)
-constexpr int kSmemBytes = 196 * 1024;   // dynamic smem per CTA
+constexpr int kSmemBytes = 100 * 1024;   // dynamic smem per CTA (two fit an SM)
 constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scratch
 
 // Row kinds (a function of n and k only).
@@ -96,23 +97,24 @@ static_assert(sizeof(RowPlan) == 64, "RowPlan layout");
 
 // Per-row state, zeroed before every call.
 struct alignas(16) RowState {
-  int32_t hticket;     // A items finished
-  int32_t fticket;     // B items finished
-  int32_t ready;       // first-level decision published
+  int32_t hticket;     // histogram items finished (radix rows)
+  int32_t fticket;     // chunk items finished (filter / copy chunks)
+  int32_t ready;       // radix rows: first-level decision published
   int32_t mode;        // kMode*
   int32_t krem;        // k still to take from the matched set
   int32_t count;       // size of the matched set
   int32_t out_count;   // output slots reserved so far
   int32_t cand_count;  // candidate entries written
   uint64_t prefix;     // composite prefix of the matched set
+  uint64_t tready;     // pre-filter rows: (1 << 32) | threshold key, one release store
   int32_t plen;        // its length in bits
-  uint32_t thresh;     // pre-filter threshold key
   int32_t src;         // phase B source: 0 = the row, 1 = its candidates
   int32_t src_len;     // entries in the phase-B source
   int32_t final_pass;  // phase B: the next filter is the last
   int32_t sb_count;    // phase B: entries compacted for the finisher
+  int32_t pad[15];
 };
-static_assert(sizeof(RowState) == 64, "RowState layout");
+static_assert(sizeof(RowState) == 128, "RowState layout");
 
 // Call header, zeroed before every call.
 struct alignas(16) Header {
@@ -159,10 +161,12 @@ struct EngineParams {
   uint64_t* sort_scratch;   // merge-sort scratch
   uint64_t* pb_sb;          // phase-B smem-bound candidates, kPhaseBSlots x kCapSB
   int32_t B;
-  int32_t CH;               // chunk length (elements), multiple of 16
+  int32_t CH;               // chunk length of single-read rows (elements), multiple of 16
+  int32_t CHR;              // chunk length of radix rows (elements), multiple of 16
   int32_t D1;               // first digit width of histogram rows
   int32_t S;                // hist ring slots
   int32_t lag;              // uniform mode: A-ahead-of-B distance
+  int32_t fin_delay;        // uniform mode: rows a FIN item trails its row
   uint32_t flags;
   uint32_t spin_limit;      // iterations of a bounded wait
   // uniform mode: every row has n = u_n, k = u_k, contiguous input,
@@ -196,15 +200,67 @@ __host__ __device__ inline int row_kind(int32_t n, int32_t k) {
   return kKindGridRadix;
 }
 __host__ __device__ inline int32_t ceil_div32(int64_t a, int64_t b) { return (int32_t)((a + b - 1) / b); }
-// Items of a row: A items run first; B items of a row depend on all of its A items.
-__host__ __device__ inline int32_t row_na(int kind, int32_t n, int32_t CH) {
-  if (kind == kKindAll || kind == kKindGridRadix) return ceil_div32(n, CH);
+// Chunk length of a row's streaming items: radix rows re-read their chunks
+// and use the short length CHR (the re-read must still be in L2); the
+// others read each chunk once and use CH.
+__host__ __device__ inline int32_t row_chunk(int kind, int32_t CH, int32_t CHR) {
+  return kind == kKindGridRadix ? CHR : CH;
+}
+// Items of a row.  A items (sample, histogram chunks, single-item rows,
+// copy chunks) run first; B items are the row's filter chunks and its finish
+// item ("FIN": resolve candidates, sort, map indices), which depends on all
+// of the row's chunk items.  A row's FIN item is placed D rows later in the
+// B sequence (inside the block of row r + D, or in a tail after the last
+// row), so that its chunks are done by the time it is claimed.
+__host__ __device__ inline int32_t row_na(int kind, int32_t n, int32_t CH, int32_t CHR) {
+  if (kind == kKindAll || kind == kKindGridRadix) return ceil_div32(n, row_chunk(kind, CH, CHR));
   return 1;
 }
-__host__ __device__ inline int32_t row_nb(int kind, int32_t n, int32_t CH) {
-  if (kind == kKindGridPref || kind == kKindGridRadix) return ceil_div32(n, CH);
+// B chunk items of a row (its FIN item not counted)
+__host__ __device__ inline int32_t row_nbc(int kind, int32_t n, int32_t CH, int32_t CHR) {
+  if (kind == kKindGridPref || kind == kKindGridRadix) return ceil_div32(n, row_chunk(kind, CH, CHR));
   return 0;
 }
+__host__ __device__ inline int32_t row_fin(int kind) {
+  return (kind == kKindGridPref || kind == kKindGridRadix || kind == kKindAll) ? 1 : 0;
+}
+// Chunk items a row's FIN item waits for.
+__host__ __device__ inline int32_t row_fin_wait(int kind, int32_t n, int32_t CH, int32_t CHR) {
+  return kind == kKindAll ? row_na(kind, n, CH, CHR) : row_nbc(kind, n, CH, CHR);
+}
+
+// B item decode for uniform batches (B rows, nc chunk items each, f = has
+// FIN, FINs delayed by D rows).  Sets row, sub (chunk index) and fin.
+__host__ __device__ inline void uniform_b_item(int64_t j, int32_t B, int32_t nc, int32_t f, int32_t D, int32_t* row,
+                                               int32_t* sub, int32_t* fin) {
+  const int64_t Dd = D < B ? D : B;
+  const int64_t head = Dd * nc;
+  const int64_t body = (int64_t)B * nc + (int64_t)f * (B - Dd);
+  if (j < head) {
+    *row = (int32_t)(j / nc);
+    *sub = (int32_t)(j % nc);
+    *fin = 0;
+  } else if (j < body) {
+    const int64_t jj = j - head;
+    const int64_t blk = nc + f;
+    const int64_t r = Dd + jj / blk;
+    const int64_t sb = jj % blk;
+    if (sb < nc) {
+      *row = (int32_t)r;
+      *sub = (int32_t)sb;
+      *fin = 0;
+    } else {
+      *row = (int32_t)(r - Dd);
+      *sub = 0;
+      *fin = 1;
+    }
+  } else {
+    *row = (int32_t)((int64_t)B - Dd + (j - body));
+    *sub = 0;
+    *fin = 1;
+  }
+}
+
 // Candidate region capacity of a row: enough for the smem finisher's set or
 // one eighth of the row, whichever is larger (never more than n).
 __host__ __device__ inline int32_t cand_capacity(int32_t n) {

@@ -67,6 +67,14 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ void st_release(int32_t* p, int32_t v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -87,6 +95,44 @@ __device__ __forceinline__ uint64_t ld_cg_u64(const uint64_t* p) {
 }
 
 __device__ __forceinline__ uint64_t shr64(uint64_t x, int s) { return s >= 64 ? 0ull : (x >> s); }
+
+// mbarrier + bulk asynchronous copy (TMA, no multicast) into this CTA's smem.
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Orders this thread's earlier generic-proxy smem accesses before later
+// async-proxy (bulk copy) writes to the same smem.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to this CTA's smem; completion is counted on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 
 // ----------------------------------------------------------------------------
 // Keys
@@ -145,7 +191,33 @@ __device__ __forceinline__ uint32_t out_key_inv(uint32_t k, bool ascend) {
 // ----------------------------------------------------------------------------
 // Shared-memory scratch at the tail of the dynamic allocation
 // ----------------------------------------------------------------------------
+// Streaming ring: kStages slots of kStageBytes at the start of smem, filled by
+// bulk copies; per-warp staging buffers behind it.
+constexpr int kStages = 5;
+constexpr int kStageBytes = 16384;
+constexpr int kStageVecs = kStageBytes / 16;
+constexpr int kRingBytes = kStages * kStageBytes;       // 80 KB
+constexpr int kSinkCand = 96;                           // filter items: candidate entries per warp
+constexpr int kSinkOut = 32;                            // filter / copy items: output entries per warp
+constexpr int kSinkPf = 128;                            // pre-filter items: candidate entries per warp
+constexpr int kSinkCandOff = kRingBytes;                // kWarps x kSinkCand x 8 B (12 KB)
+constexpr int kSinkOutOff = kSinkCandOff + kWarps * kSinkCand * 8;  // kWarps x kSinkOut x 8 B (4 KB)
+constexpr int kSinkPfOff = kRingBytes;                  // kWarps x kSinkPf x 8 B (16 KB)
+constexpr int kHistOff = kRingBytes;                    // first-digit histogram (<= 16 KB)
+constexpr int kResolveHistOff = kCapSB * 8;             // 4096-bin histogram behind a finisher's entries
+constexpr int kSmemRowHistOff = kSmemRowCap * 4;        // behind an smem row's values
+constexpr int kSampleHistOff = kSampleMax * 4;          // behind the sampled keys
+static_assert(kSinkPfOff + kWarps * kSinkPf * 8 <= kSmemBytes - kMiscBytes, "pre-filter smem");
+static_assert(kSinkOutOff + kWarps * kSinkOut * 8 <= kSmemBytes - kMiscBytes, "filter smem");
+static_assert(kHistOff + (4 << kMaxD1) <= kSmemBytes - kMiscBytes, "histogram smem");
+static_assert(kResolveHistOff + 16384 <= kSmemBytes - kMiscBytes, "finisher smem");
+static_assert(kSmemRowHistOff + kCapSort * 8 <= kSmemBytes - kMiscBytes, "smem-row sort area");
+static_assert(kSampleHistOff + 16384 <= kSmemBytes - kMiscBytes, "sample smem");
+static_assert(kCapSort * 8 <= kSmemBytes - kMiscBytes, "sort smem");
+
 struct Misc {
+  uint64_t mbar[kStages];        // ring slot filled (bulk copy bytes landed)
+  uint64_t mbar_empty[kStages];  // ring slot drained (every warp is done with it)
   uint32_t hist256[256];
   uint32_t scan[64];
   int32_t next_q;
@@ -158,6 +230,12 @@ struct Misc {
   uint64_t st_prefix;
   int32_t st_candn;
   int32_t pad[7];
+  uint64_t red_lo, red_hi;
+  uint64_t red_hi_w[32];
+  int32_t rel_row;     // row whose chunk counter the next iteration releases (-1: none)
+  int32_t t_row;       // row of the cached pre-filter threshold (-1: none)
+  uint32_t t_val;      // the cached threshold
+  int32_t ring_dirty;  // the ring's smem was written by a non-streaming item
   int32_t pbtab[200];  // phase-B row table (row ids, chunk counts, prefix)
 };
 static_assert(sizeof(Misc) <= kMiscBytes, "Misc too large");
@@ -181,7 +259,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* scan, 
   if (lane == 31) scan[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = scan[lane];
+    uint32_t w = lane < kWarps ? scan[lane] : 0u;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(kFull, w, o);
@@ -287,8 +365,8 @@ __device__ inline void block_bitonic_sort(uint64_t* s, int n) {
 // ----------------------------------------------------------------------------
 struct RowCtx {
   int64_t in_off, out_off, cand_off, sort_off;
-  int32_t n, k, a0, b0, na, nb, cand_cap, slot_use;
-  int32_t kind, IB;
+  int32_t n, k, a0, b0, na, nbc, fin_wait, cand_cap, slot_use;
+  int32_t kind, IB, ch;
   uint32_t flip;
   float scaler;
 };
@@ -302,10 +380,10 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
     c.in_off = (int64_t)r * p.u_n;
     c.out_off = (int64_t)r * p.u_k;
     c.kind = row_kind(c.n, c.k);
-    c.na = row_na(c.kind, c.n, p.CH);
-    c.nb = row_nb(c.kind, c.n, p.CH);
+    c.na = row_na(c.kind, c.n, p.CH, p.CHR);
+    c.nbc = row_nbc(c.kind, c.n, p.CH, p.CHR);
     c.a0 = r * c.na;
-    c.b0 = r * c.nb;
+    c.b0 = 0;  // uniform batches decode B items arithmetically
     c.cand_cap = p.u_cand_cap;
     c.cand_off = (int64_t)r * p.u_cand_cap;
     c.sort_off = p.u_sort_cap ? (int64_t)r * p.u_sort_cap : -1;
@@ -319,14 +397,16 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
     c.n = pl.n;
     c.k = pl.k;
     c.kind = row_kind(c.n, c.k);
-    c.na = row_na(c.kind, c.n, p.CH);
-    c.nb = row_nb(c.kind, c.n, p.CH);
+    c.na = row_na(c.kind, c.n, p.CH, p.CHR);
+    c.nbc = row_nbc(c.kind, c.n, p.CH, p.CHR);
     c.a0 = pl.a0;
     c.b0 = pl.b0;
     c.cand_cap = pl.cand_cap;
     c.slot_use = pl.slot_use;
   }
   c.IB = index_bits(c.n);
+  c.ch = row_chunk(c.kind, p.CH, p.CHR);
+  c.fin_wait = row_fin_wait(c.kind, c.n, p.CH, p.CHR);
   c.flip = (p.flags & kFlagLargest) ? KT<VT, SCALE>::KMASK : 0u;
   c.scaler = 0.f;
   if constexpr (SCALE) {
@@ -488,24 +568,71 @@ __device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint
 // ----------------------------------------------------------------------------
 // Shared-memory selection
 // ----------------------------------------------------------------------------
-// The r-th smallest (1-based) of cnt KB-bit keys in shared memory.
+// Block-wide min of lo and max of hi over all threads (pass ~0 / 0 to abstain).
+__device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t* mn, uint64_t* mx, Misc* m) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)lo, o));
+    hi = max(hi, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)hi, o));
+  }
+  uint64_t* red = reinterpret_cast<uint64_t*>(m->scan);  // 64 x u32 = 32 x u64
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) {
+    red[warp] = lo;
+    m->red_hi_w[warp] = hi;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t a = lane < kWarps ? red[lane] : ~0ull, b = lane < kWarps ? m->red_hi_w[lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = min(a, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)a, o));
+      b = max(b, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)b, o));
+    }
+    if (lane == 0) {
+      m->red_lo = a;
+      m->red_hi = b;
+    }
+  }
+  __syncthreads();
+  *mn = m->red_lo;
+  *mx = m->red_hi;
+  __syncthreads();
+}
+
+// Threshold key of a sample: the r-th smallest (1-based) of cnt KB-bit keys
+// in shared memory, or an upper bound of it.  The bits every key shares are
+// skipped (min/max reduction); then at most two 12-bit digits refine it.
+// When bits remain after that, the upper edge of the r-th key's bin is
+// returned (at least r keys are <= it).  hist: 4096 counters of smem.
 template <int KB>
-__device__ uint32_t block_kth_key(const uint32_t* keys, int cnt, int r, Misc* m, int32_t* status) {
-  uint32_t prefix = 0;
-  int plen = 0;
+__device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r, uint32_t* hist, Misc* m,
+                                           int32_t* status) {
+  uint64_t lo = ~0ull, hi = 0;
+  for (int i = threadIdx.x; i < cnt; i += kThreads) {
+    lo = min(lo, (uint64_t)keys[i]);
+    hi = max(hi, (uint64_t)keys[i]);
+  }
+  uint64_t mn, mx;
+  block_minmax(lo, hi, &mn, &mx, m);
+  if (mn >= mx) return (uint32_t)mn;
+  int plen = __clzll((long long)(mn ^ mx)) - (64 - KB);  // shared leading bits
+  uint32_t prefix = plen > 0 ? (uint32_t)(mn >> (KB - plen)) : 0u;
   uint32_t krem = (uint32_t)r;
-  while (plen < KB) {
-    const int D = min(8, KB - plen);
-    for (int i = threadIdx.x; i < 256; i += kThreads) m->hist256[i] = 0;
+  for (int level = 0; level < 2 && plen < KB; ++level) {
+    const int D = min(12, KB - plen);
+    const int NB = 1 << D;
+    for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
     __syncthreads();
     const int sd = KB - plen - D;
     for (int i = threadIdx.x; i < cnt; i += kThreads) {
       const uint32_t k = keys[i];
       const bool match = plen == 0 || (k >> (KB - plen)) == prefix;
-      if (match) atomicAdd(&m->hist256[(k >> sd) & ((1u << D) - 1u)], 1u);
+      if (match) atomicAdd(&hist[(k >> sd) & (uint32_t)(NB - 1)], 1u);
     }
     __syncthreads();
-    block_select<false>(m->hist256, 1 << D, krem, m);
+    block_select<false>(hist, NB, krem, m);
     if (!m->sel_found) {
       if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
       return (uint32_t)(((uint64_t)1 << KB) - 1);
@@ -515,38 +642,63 @@ __device__ uint32_t block_kth_key(const uint32_t* keys, int cnt, int r, Misc* m,
     krem -= m->sel_cum;
     __syncthreads();
   }
-  return prefix;
+  if (plen >= KB) return prefix;
+  return (uint32_t)(((uint64_t)prefix << (KB - plen)) | (((uint64_t)1 << (KB - plen)) - 1));
 }
 
 // Entries get(i) -> (bits, pos), all matching (prefix, plen).  Refines the
-// prefix with 8-bit digits over the composite (key << IB | pos) until the
-// matched set size equals krem.  On return the selected entries are those
-// whose composite prefix is <= prefix.
+// prefix over the composite (key << IB | pos) until the matched set size
+// equals krem: first past the bits all entries share (min/max reduction),
+// then with 12-bit digits (hist: 4096 counters of smem).  On return the
+// selected entries are those whose composite prefix is <= prefix.
 template <int VT, bool SCALE, typename G>
 __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix, int& plen, int& krem, int count,
-                             Misc* m, int32_t* status) {
+                             uint32_t* hist, Misc* m, int32_t* status) {
   using K = KT<VT, SCALE>;
   const int W = K::KB + rc.IB;
-  while (count != krem) {
-    if (plen >= W || count < krem) {
-      if (threadIdx.x == 0) atomicOr(status, kStatusLevels);
-      break;
-    }
-    const int D = min(8, W - plen);
-    for (int i = threadIdx.x; i < 256; i += kThreads) m->hist256[i] = 0;
-    __syncthreads();
-    const int sh = W - plen;
-    const int sd = W - plen - D;
-    const uint32_t dm = (1u << D) - 1u;
+  if (count != krem && cnt > 0) {
+    uint64_t lo = ~0ull, hi = 0;
     for (int i = threadIdx.x; i < cnt; i += kThreads) {
       uint32_t bits;
       int64_t pos;
       get(i, bits, pos);
       const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
-      if (shr64(c, sh) == prefix) atomicAdd(&m->hist256[(uint32_t)shr64(c, sd) & dm], 1u);
+      if (shr64(c, W - plen) == prefix) {
+        lo = min(lo, c);
+        hi = max(hi, c);
+      }
+    }
+    uint64_t mn, mx;
+    block_minmax(lo, hi, &mn, &mx, m);
+    if (mn != ~0ull) {
+      const int common = (mn == mx) ? W : (__clzll((long long)(mn ^ mx)) - (64 - W));
+      if (common > plen) {
+        plen = common;
+        prefix = shr64(mn, W - plen);
+      }
+    }
+  }
+  while (count != krem) {
+    if (plen >= W || count < krem) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusLevels);
+      break;
+    }
+    const int D = min(12, W - plen);
+    const int NB = 1 << D;
+    for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
+    __syncthreads();
+    const int sh = W - plen;
+    const int sd = W - plen - D;
+    const uint32_t dm = (uint32_t)NB - 1u;
+    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+      uint32_t bits;
+      int64_t pos;
+      get(i, bits, pos);
+      const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
+      if (shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
     }
     __syncthreads();
-    block_select<false>(m->hist256, 1 << D, (uint32_t)krem, m);
+    block_select<false>(hist, NB, (uint32_t)krem, m);
     if (!m->sel_found) {
       if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
       break;
@@ -604,6 +756,8 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
   const int64_t kk = min((int64_t)rc.n, (int64_t)rc.k);
   const bool idx64 = (p.flags & kFlagIdx64) != 0;
   const bool withidx = (p.flags & kFlagWithIdxIn) != 0;
+  const bool sorting = (p.flags & kFlagSorted) && kk > 1;
+  if (!sorting && !withidx && kk == rc.k) return;  // unsorted, positions, no idle slots: nothing to do
   __threadfence();
   __syncthreads();
   auto load_pos = [&](int64_t i) -> int64_t {
@@ -743,14 +897,129 @@ struct Engine {
   static constexpr int ES = K::ES;
   static constexpr int VEC = K::VEC;
   static constexpr int U = 4;
-  static constexpr int kSinkCand = 256;  // candidate entries per warp buffer
-  static constexpr int kSinkOut = 64;    // output entries per warp buffer
 
   const EngineParams& p;
   uint8_t* smem;
   Misc* m;
+  uint32_t gstage = 0;  // ring stages consumed so far by this CTA (uniform)
+  int pending_rel = -1; // row whose chunk counter is still to be released (uniform)
+
+  // Releases the previous chunk item's completion on its row's counter: one
+  // thread fences (the item's writes by all warps precede it through the
+  // item's closing barrier) and increments.  Called where that thread's
+  // stall overlaps other work: after a streaming item's first copies and
+  // threshold wait, or at the start of a non-streaming item.
+  __device__ void do_release() {
+    if (pending_rel >= 0) {
+      if (threadIdx.x == kThreads - 32) {
+        __threadfence();
+        atomicAdd(&p.rs[pending_rel].fticket, 1);
+      }
+      pending_rel = -1;
+    }
+  }
 
   __device__ Engine(const EngineParams& p_, uint8_t* s) : p(p_), smem(s), m(misc_of(s)) {}
+
+  __device__ uint64_t* cand_sink(int warp) const {
+    return reinterpret_cast<uint64_t*>(smem + kSinkCandOff) + warp * kSinkCand;
+  }
+  __device__ uint64_t* out_sink(int warp) const {
+    return reinterpret_cast<uint64_t*>(smem + kSinkOutOff) + warp * kSinkOut;
+  }
+
+  // Streams positions [a, b) of a row.  The aligned middle travels through
+  // the smem ring in bulk copies of kStageBytes issued by thread 0, up to
+  // kStages in flight; every thread consumes two 16-byte vectors per stage
+  // with fv(x, pos0, ok).  A slot is refilled once all 32 warps have
+  // arrived on its "empty" barrier, so no block-wide barrier per stage.  The
+  // unaligned head and tail (< 16 bytes each) go through fe(bits, pos, ok).
+  // pre() runs once the first copies are in flight (e.g. to wait for a
+  // row's threshold).  All callbacks are called warp-uniformly.
+  template <typename PRE, typename FE, typename FV>
+  __device__ void stream_chunk(const RowCtx& rc, int64_t a, int64_t b, PRE&& pre, FE&& fe, FV&& fv) {
+    const char* row = static_cast<const char*>(p.val_in) + rc.in_off * ES;
+    int64_t head = 0, nvec = 0, va = a;
+    if (b > a) {
+      const uintptr_t addr_a = reinterpret_cast<uintptr_t>(row + a * ES);
+      head = (int64_t)(((16u - (unsigned)(addr_a & 15u)) & 15u) / ES);
+      if (head > b - a) head = b - a;
+      va = a + head;
+      nvec = (b - va) / VEC;
+    }
+    const int64_t vb = va + nvec * VEC;
+    const int64_t tail = b > a ? b - vb : 0;
+    const uint4* src = reinterpret_cast<const uint4*>(row + va * ES);
+    const int64_t nst = (nvec + kStageVecs - 1) / kStageVecs;
+    uint4* ring = reinterpret_cast<uint4*>(smem);
+    // thread 0 only: fill the slot of stage i once its previous use drained
+    auto issue = [&](int64_t i) {
+      const uint32_t g = gstage + (uint32_t)i;
+      const uint32_t slot = g % kStages;
+      if (g >= (uint32_t)kStages) {
+        const uint32_t parity = ((g / kStages) - 1u) & 1u;
+        uint32_t it = 0;
+        while (!mbar_try_wait(&m->mbar_empty[slot], parity)) {
+          if (++it > p.spin_limit) {
+            atomicOr(&p.hdr->status, kStatusTimeout);
+            break;
+          }
+        }
+      }
+      const int64_t v0 = i * kStageVecs;
+      const uint32_t bytes = (uint32_t)min((int64_t)kStageVecs, nvec - v0) * 16u;
+      mbar_expect_tx(&m->mbar[slot], bytes);
+      bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &m->mbar[slot]);
+    };
+    if (threadIdx.x == 0 && nst > 0) {
+      // a non-streaming item may have written this smem through the generic
+      // proxy: order that before the bulk copies overwrite it
+      if (m->ring_dirty) {
+        fence_proxy_async();
+        m->ring_dirty = 0;
+      }
+      for (int64_t i = 0; i < min(nst, (int64_t)kStages); ++i) issue(i);
+    }
+    pre();
+    do_release();
+    if (head > 0 || tail > 0) {
+      const int t = threadIdx.x;
+      const bool vh = t < head, vt = t < tail;
+      uint32_t bh = 0, bt = 0;
+      if (vh) bh = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[a + t]
+                           : (uint32_t)reinterpret_cast<const unsigned short*>(row)[a + t];
+      if (vt) bt = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[vb + t]
+                           : (uint32_t)reinterpret_cast<const unsigned short*>(row)[vb + t];
+      if (head > 0) fe(bh, a + t, vh);
+      if (tail > 0) fe(bt, vb + t, vt);
+    }
+    for (int64_t i = 0; i < nst; ++i) {
+      const uint32_t g = gstage + (uint32_t)i;
+      const uint32_t slot = g % kStages;
+      const uint32_t parity = (g / kStages) & 1u;
+      uint32_t it = 0;
+      while (!mbar_try_wait(&m->mbar[slot], parity)) {
+        if (++it > p.spin_limit) {
+          if (threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusTimeout);
+          break;
+        }
+      }
+      const int64_t v0 = i * kStageVecs;
+      const int cnt = (int)min((int64_t)kStageVecs, nvec - v0);
+      const uint4* st = ring + (size_t)slot * kStageVecs;
+#pragma unroll
+      for (int j = 0; j < kStageVecs / kThreads; ++j) {
+        const int v = j * kThreads + threadIdx.x;
+        const bool ok = v < cnt;
+        const uint4 x = ok ? st[v] : make_uint4(0, 0, 0, 0);
+        fv(x, va + (v0 + v) * VEC, ok);
+      }
+      __syncwarp();
+      if ((threadIdx.x & 31) == 0) mbar_arrive(&m->mbar_empty[slot]);
+      if (threadIdx.x == 0 && i + kStages < nst) issue(i + kStages);
+    }
+    gstage += (uint32_t)nst;
+  }
 
   __device__ bool spin_until_ge(const uint32_t* addr, uint32_t target) {
     for (uint32_t it = 0; it < p.spin_limit; ++it) {
@@ -784,7 +1053,8 @@ struct Engine {
       keys[j] = key_of(load_bits(rc, pos), rc);
     }
     __syncthreads();
-    const uint32_t t = block_kth_key<K::KB>(keys, S, sample_rank(rc.n, rc.k, S), m, &p.hdr->status);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
+    const uint32_t t = block_sample_threshold<K::KB>(keys, S, sample_rank(rc.n, rc.k, S), hist, m, &p.hdr->status);
     __syncthreads();
     return t;
   }
@@ -808,9 +1078,10 @@ struct Engine {
       bits = vals[i];
       pos = i;
     };
-    smem_resolve<VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, m, &p.hdr->status);
+    smem_resolve<VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
+                            &p.hdr->status);
     smem_emit<VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m);
-    post_process<VT, SCALE>(p, rc, smem + 65536, m);
+    post_process<VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
   }
 
   // ---- one CTA, the whole row from global memory (n <= kCtaRowCap)
@@ -870,7 +1141,8 @@ struct Engine {
       if (c >= rc.k && c <= kCapSB) {
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, m, &p.hdr->status);
+        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+                                &p.hdr->status);
         smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
         post_process<VT, SCALE>(p, rc, smem, m);
         return;
@@ -916,89 +1188,184 @@ struct Engine {
     if (!final_mode) {
       const int ne = min((int)m->counter, kCapSB);
       __syncthreads();
-      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+                              &p.hdr->status);
       smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
     }
     post_process<VT, SCALE>(p, rc, smem, m);
   }
 
   // ---- copy chunk ia of a k >= n row (every element is selected)
-  __device__ bool all_item(int r, const RowCtx& rc, int ia) {
+  __device__ void all_item(int r, const RowCtx& rc, int ia) {
     RowState* rs = p.rs + r;
     const int warp = threadIdx.x >> 5;
-    WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + warp * kSinkOut, 0};
+    WarpBuf ob{out_sink(warp), 0};
     uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
     auto fl = [&](const WarpBuf& s) { flush_out<VT>(p, s, ctr, rc.out_off, rc.k); };
-    const int64_t a = (int64_t)ia * p.CH, b = min((int64_t)rc.n, a + p.CH);
-    for_range_v<ES, U>(
-        p.val_in, rc.in_off, a, b,
+    const int64_t a = (int64_t)ia * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
+    stream_chunk(
+        rc, a, b, [] {},
         [&](uint32_t bits, int64_t pos, bool ok) { sink_push(ob, kSinkOut, ok, make_entry(bits, pos), fl); },
         [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
           for (int e = 0; e < VEC; ++e) sink_push(ob, kSinkOut, ok, make_entry(vec_elem<ES>(x, e), pos0 + e), fl);
         });
     if (ob.n) fl(ob);
-    __threadfence();
+    defer_release(r);
+  }
+
+  // A chunk item's completion is counted on the row's fticket by one
+  // thread after the item's closing barrier, without waiting for the result
+  // (the release's latency overlaps the next item).
+  __device__ void defer_release(int r) {
+    if (threadIdx.x == 0) m->rel_row = r;
+  }
+
+  // ---- FIN item: wait for the row's chunk items, then finish the row
+  __device__ void fin_item(int r, const RowCtx& rc) {
+    if (threadIdx.x == 0) {
+      const int32_t* t = &p.rs[r].fticket;
+      uint32_t it = 0;
+      while (ld_acquire(t) < rc.fin_wait) {
+        if (++it > p.spin_limit) {
+          atomicOr(&p.hdr->status, kStatusTimeout);
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
     __syncthreads();
-    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
-    __syncthreads();
-    return m->bcast2 != 0;
+    finish_row(r);
   }
 
   // ---- sample item of a pre-filter row: publish the threshold
   __device__ void sample_item(int r, const RowCtx& rc) {
     const uint32_t T = sample_threshold(rc);
-    if (threadIdx.x == 0) {
-      RowState* rs = p.rs + r;
-      rs->thresh = T;
-      __threadfence();
-      st_release(&rs->ready, 1);
-    }
+    if (threadIdx.x == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
   }
 
-  // ---- filter item of a pre-filter row: keys <= T into the candidates
-  __device__ bool pf_item(int r, const RowCtx& rc, int ib) {
+  // ---- filter item of a pre-filter row: keys <= T into the candidates.
+  // Hot loop: a float (or half2) compare against the threshold's value with
+  // the unordered predicate, so NaN always passes; it keeps a superset of
+  // the keys <= T.  Only vectors with a passing element take the exact
+  // integer-key test and the warp-scan compaction into the warp's buffer.
+  template <bool LARGEST>
+  __device__ void pf_item_t(int r, const RowCtx& rc, int ib) {
     RowState* rs = p.rs + r;
-    if (threadIdx.x == 0) {
-      uint32_t t = 0;
-      if (spin_until_ge(reinterpret_cast<const uint32_t*>(&rs->ready), 1u)) t = __ldcg(&rs->thresh);
-      else t = 0u;  // timed out: keep nothing (the status bit reports it)
-      m->st_prefix = t;
-    }
-    __syncthreads();
-    const uint32_t T = (uint32_t)m->st_prefix;
+    uint32_t T = 0;
+    auto pre = [&]() {
+      if (threadIdx.x == 0 && m->t_row != r) {
+        uint64_t v = ld_acquire_u64(&rs->tready);
+        for (uint32_t it = 0; !(v >> 32); ++it) {
+          if (it > p.spin_limit) {
+            atomicOr(&p.hdr->status, kStatusTimeout);  // only keys <= 0 pass then
+            break;
+          }
+          __nanosleep(64);
+          v = ld_acquire_u64(&rs->tready);
+        }
+        m->t_val = (uint32_t)v;
+        m->t_row = r;
+      }
+      __syncthreads();
+      T = m->t_val;
+    };
     const int warp = threadIdx.x >> 5;
-    WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
+    const unsigned lane = threadIdx.x & 31u;
+    constexpr int kCap = kSinkPf;
+    WarpBuf cb{reinterpret_cast<uint64_t*>(smem + kSinkPfOff) + warp * kCap, 0};
     uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
     uint64_t* dst = p.cand + rc.cand_off;
-    auto fl = [&](const WarpBuf& s) { flush_cand(s, ctr, dst, rc.cand_cap, &p.hdr->status); };
-    const int64_t a = (int64_t)ib * p.CH, b = min((int64_t)rc.n, a + p.CH);
     const uint32_t flip = rc.flip;
     const float sc = rc.scaler;
-    for_range_v<ES, U>(
-        p.val_in, rc.in_off, a, b,
+    const int64_t a = (int64_t)ib * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
+    // lane's hit mask over up to VEC elements -> warp buffer
+    auto push = [&](uint32_t hm, uint32_t e0bits_unused, auto elem_bits, int64_t pos0) {
+      (void)e0bits_unused;
+      const uint32_t h = (uint32_t)__popc(hm);
+      uint32_t x = h;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= (unsigned)o) x += y;
+      }
+      const uint32_t tot = __shfl_sync(kFull, x, 31);
+      if (cb.n + tot > (uint32_t)kCap) {
+        __syncwarp();
+        flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+        cb.n = 0;
+        __syncwarp();
+      }
+      uint32_t w = cb.n + x - h;
+      for (uint32_t mm = hm; mm; mm &= mm - 1) {
+        const int e = __ffs(mm) - 1;
+        cb.buf[w++] = make_entry(elem_bits(e), pos0 + e);
+      }
+      cb.n += tot;
+    };
+    stream_chunk(
+        rc, a, b, pre,
         [&](uint32_t bits, int64_t pos, bool ok) {
-          sink_push(cb, kSinkCand, ok && sel_key<VT, SCALE>(bits, flip, sc) <= T, make_entry(bits, pos), fl);
+          const bool hit = ok && sel_key<VT, SCALE>(bits, flip, sc) <= T;
+          if (__any_sync(kFull, hit)) push(hit ? 1u : 0u, 0u, [&](int) { return bits; }, pos);
         },
         [&](const uint4& x, int64_t pos0, bool ok) {
-          bool hit[VEC];
-          bool any = false;
+          // threshold as a value (computed here so it is live only in the loop)
+          const uint32_t ukT = LARGEST ? (~T & K::KMASK) : T;
+          bool any;
+          if constexpr (SCALE) {
+            const float tv = __uint_as_float(unkey32(ukT));
+            any = false;
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            hit[e] = ok && sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) <= T;
-            any |= hit[e];
+            for (int e = 0; e < VEC; ++e) {
+              const float d = __fsub_rn(to_float<VT>(vec_elem<ES>(x, e)), sc);
+              any |= LARGEST ? !(d < tv) : !(d > tv);
+            }
+          } else if constexpr (VT == kF32) {
+            const float tv = __uint_as_float(unkey32(ukT));
+            const float f0 = __uint_as_float(x.x), f1 = __uint_as_float(x.y);
+            const float f2 = __uint_as_float(x.z), f3 = __uint_as_float(x.w);
+            if (LARGEST) any = !(f0 < tv) | !(f1 < tv) | !(f2 < tv) | !(f3 < tv);
+            else any = !(f0 > tv) | !(f1 > tv) | !(f2 > tv) | !(f3 > tv);
+          } else {
+            const uint32_t tb = unkey16(ukT);
+            const uint32_t t2 = tb | (tb << 16);
+            uint32_t mk;
+            if constexpr (VT == kF16) {
+              const __half2 th = *reinterpret_cast<const __half2*>(&t2);
+              const __half2 h0 = *reinterpret_cast<const __half2*>(&x.x), h1 = *reinterpret_cast<const __half2*>(&x.y);
+              const __half2 h2 = *reinterpret_cast<const __half2*>(&x.z), h3 = *reinterpret_cast<const __half2*>(&x.w);
+              mk = LARGEST ? (__hgeu2_mask(h0, th) | __hgeu2_mask(h1, th) | __hgeu2_mask(h2, th) | __hgeu2_mask(h3, th))
+                           : (__hleu2_mask(h0, th) | __hleu2_mask(h1, th) | __hleu2_mask(h2, th) | __hleu2_mask(h3, th));
+            } else {
+              const __nv_bfloat162 th = *reinterpret_cast<const __nv_bfloat162*>(&t2);
+              const __nv_bfloat162 h0 = *reinterpret_cast<const __nv_bfloat162*>(&x.x);
+              const __nv_bfloat162 h1 = *reinterpret_cast<const __nv_bfloat162*>(&x.y);
+              const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&x.z);
+              const __nv_bfloat162 h3 = *reinterpret_cast<const __nv_bfloat162*>(&x.w);
+              mk = LARGEST ? (__hgeu2_mask(h0, th) | __hgeu2_mask(h1, th) | __hgeu2_mask(h2, th) | __hgeu2_mask(h3, th))
+                           : (__hleu2_mask(h0, th) | __hleu2_mask(h1, th) | __hleu2_mask(h2, th) | __hleu2_mask(h3, th));
+            }
+            any = mk != 0;
           }
+          any = any && ok;
           if (__any_sync(kFull, any)) {
+            uint32_t hm = 0;
+            if (any) {
 #pragma unroll
-            for (int e = 0; e < VEC; ++e) sink_push(cb, kSinkCand, hit[e], make_entry(vec_elem<ES>(x, e), pos0 + e), fl);
+              for (int e = 0; e < VEC; ++e)
+                if (sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) <= T) hm |= 1u << e;
+            }
+            push(hm, 0u, [&](int e) { return vec_elem<ES>(x, e); }, pos0);
           }
         });
-    if (cb.n) fl(cb);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->fticket, 1) == rc.nb - 1;
-    __syncthreads();
-    return m->bcast2 != 0;
+    if (cb.n) flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+    defer_release(r);
+  }
+
+  __device__ void pf_item(int r, const RowCtx& rc, int ib) {
+    if (p.flags & kFlagLargest) pf_item_t<true>(r, rc, ib);
+    else pf_item_t<false>(r, rc, ib);
   }
 
   // ---- histogram item of a radix row: first digit of chunk ia
@@ -1007,19 +1374,19 @@ struct Engine {
     const int NB = 1 << D1;
     const int s = rc.slot_use % p.S;
     const uint32_t use = (uint32_t)(rc.slot_use / p.S);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kHistOff);
     uint32_t* ghist = p.hist_ring + (size_t)s * ((size_t)1 << kMaxD1);
     if (threadIdx.x == 0) m->bcast = use == 0 ? 1 : (int)spin_until_ge(p.slot_gen + s, use);
     for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) *reinterpret_cast<uint4*>(hist + i) = make_uint4(0, 0, 0, 0);
     __syncthreads();
     const bool slot_ok = m->bcast != 0;
     const int shift = K::KB - D1;
-    const int64_t a = (int64_t)ia * p.CH, b = min((int64_t)rc.n, a + p.CH);
+    const int64_t a = (int64_t)ia * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
     const uint32_t flip = rc.flip;
     const float sc = rc.scaler;
     bool agg = false;
-    for_range_v<ES, U>(
-        p.val_in, rc.in_off, a, b,
+    stream_chunk(
+        rc, a, b, [] {},
         [&](uint32_t bits, int64_t, bool ok) { hist_add_agg(hist, sel_key<VT, SCALE>(bits, flip, sc) >> shift, ok); },
         [&](const uint4& x, int64_t, bool ok) {
 #pragma unroll
@@ -1076,7 +1443,7 @@ struct Engine {
   }
 
   // ---- filter item of a radix row
-  __device__ bool f_item(int r, const RowCtx& rc, int ib) {
+  __device__ void f_item(int r, const RowCtx& rc, int ib) {
     RowState* rs = p.rs + r;
     if (threadIdx.x == 0) {
       int mode = kModeNone;
@@ -1091,8 +1458,8 @@ struct Engine {
       const int shift = K::KB - p.D1;
       const bool final_mode = mode == kModeFinal;
       const int warp = threadIdx.x >> 5;
-      WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
-      WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + kWarps * kSinkCand + warp * kSinkOut, 0};
+      WarpBuf cb{cand_sink(warp), 0};
+      WarpBuf ob{out_sink(warp), 0};
       uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
       uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
       uint64_t* dst = p.cand + rc.cand_off;
@@ -1107,8 +1474,8 @@ struct Engine {
         sink_push(ob, kSinkOut, to_out, make_entry(bits, pos), flo);
         sink_push(cb, kSinkCand, to_cand, make_entry(bits, pos), flc);
       };
-      const int64_t a = (int64_t)ib * p.CH, b = min((int64_t)rc.n, a + p.CH);
-      for_range_v<ES, U>(p.val_in, rc.in_off, a, b, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      const int64_t a = (int64_t)ib * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
+      stream_chunk(rc, a, b, [] {}, one, [&](const uint4& x, int64_t pos0, bool ok) {
         bool any = false;
 #pragma unroll
         for (int e = 0; e < VEC; ++e) any |= ok && (sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) >> shift) <= prefix;
@@ -1120,11 +1487,8 @@ struct Engine {
       if (ob.n) flo(ob);
       if (cb.n) flc(cb);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->fticket, 1) == rc.nb - 1;
-    __syncthreads();
-    return m->bcast2 != 0;
+    do_release();  // the previous item's counter, if no stream ran above
+    defer_release(r);
   }
 
   // Hands a row to phase B.
@@ -1173,7 +1537,8 @@ struct Engine {
         __syncthreads();
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, m, &p.hdr->status);
+        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+                                &p.hdr->status);
         smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
         post_process<VT, SCALE>(p, rc, smem, m);
       } else if (c >= rc.k && c <= rc.cand_cap) {
@@ -1190,7 +1555,8 @@ struct Engine {
       uint64_t prefix = m->st_prefix;
       int plen = m->st_plen, krem = m->st_krem;
       __syncthreads();
-      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+                              &p.hdr->status);
       smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
       post_process<VT, SCALE>(p, rc, smem, m);
     } else if (mode == kModeCand) {
@@ -1259,8 +1625,11 @@ struct Engine {
       const int nL = __ldcg(&p.hdr->nlarge);
       if (nL <= 0) return;
       const int nG = min(nL, kPhaseBSlots);
-      // rows already small enough skip the histogram
+      // rows already small enough skip the histogram; each row's histogram
+      // slot is cleared here (the call clears the ring only for radix rows)
       for (int i = blockIdx.x; i < nG; i += gridDim.x) {
+        uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
+        for (int j = threadIdx.x; j < 4096; j += kThreads) gh[j] = 0;
         if (threadIdx.x == 0) {
           RowState* rs = p.rs + p.large_list[i];
           const int cnt = __ldcg(&rs->count), kr = __ldcg(&rs->krem);
@@ -1349,8 +1718,8 @@ struct Engine {
         const bool final_mode = __ldcg(&rs->count) == __ldcg(&rs->krem);
         const int W = K::KB + rc.IB;
         const int sh = W - plen;
-        WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kSinkCand, 0};
-        WarpBuf ob{reinterpret_cast<uint64_t*>(smem) + kWarps * kSinkCand + warp * kSinkOut, 0};
+        WarpBuf cb{cand_sink(warp), 0};
+        WarpBuf ob{out_sink(warp), 0};
         uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->sb_count);
         uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
         uint64_t* dst = p.pb_sb + (size_t)i * kCapSB;
@@ -1388,7 +1757,8 @@ struct Engine {
             bits = (uint32_t)(e >> 32);
             pos = (int64_t)(uint32_t)e;
           };
-          smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, m, &p.hdr->status);
+          smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+                              &p.hdr->status);
           smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
         }
         post_process<VT, SCALE>(p, rc, smem, m);
@@ -1440,16 +1810,31 @@ __device__ __forceinline__ bool decode_item(int q, int NA, int NB, int L, int& i
 }
 
 template <int VT, bool SCALE>
-__global__ void __launch_bounds__(kThreads, 1) engine_kernel(const __grid_constant__ EngineParams p) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __grid_constant__ EngineParams p) {
   extern __shared__ __align__(16) uint8_t smem[];
   Engine<VT, SCALE> e(p, smem);
   Misc* m = e.m;
   if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&m->mbar[i], 1);
+      mbar_init(&m->mbar_empty[i], kWarps);
+    }
+    mbar_fence_init();
+    m->rel_row = -1;
+    m->t_row = -1;
+    m->ring_dirty = 0;
+  }
+  __syncthreads();
   int NA, NB, lag;
+  int ukind = 0, una = 1, unc = 0, ufin = 0;
   if (p.uniform) {
-    const int kind = row_kind(p.u_n, p.u_k);
-    NA = p.B * row_na(kind, p.u_n, p.CH);
-    NB = p.B * row_nb(kind, p.u_n, p.CH);
+    ukind = row_kind(p.u_n, p.u_k);
+    una = row_na(ukind, p.u_n, p.CH, p.CHR);
+    unc = row_nbc(ukind, p.u_n, p.CH, p.CHR);
+    ufin = row_fin(ukind);
+    NA = p.B * una;
+    NB = p.B * (unc + ufin);
     lag = p.lag;
   } else {
     NA = __ldcg(&p.hdr->na);
@@ -1460,55 +1845,63 @@ __global__ void __launch_bounds__(kThreads, 1) engine_kernel(const __grid_consta
   if (threadIdx.x == 0) m->next_q = (int)atomicAdd(&p.hdr->qhead, 1u);
   __syncthreads();
   int q = m->next_q;
-  int pending = -1;
-  while (true) {
-    if (q >= NQ) {
-      if (pending >= 0) e.finish_row(pending);
-      break;
-    }
+  while (q < NQ) {
+    // the previous chunk item's counter is released during this item
+    e.pending_rel = m->rel_row;
     __syncthreads();
-    const bool prefetch = pending < 0;
+    if (threadIdx.x == 0) m->rel_row = -1;
     uint32_t nq = 0;
-    if (threadIdx.x == 0 && prefetch) nq = atomicAdd(&p.hdr->qhead, 1u);
+    if (threadIdx.x == 0) nq = atomicAdd(&p.hdr->qhead, 1u);
     int idx;
     const bool isA = decode_item(q, NA, NB, lag, idx);
-    int r;
-    if (p.uniform) {
-      const int kind = row_kind(p.u_n, p.u_k);
-      r = isA ? idx / row_na(kind, p.u_n, p.CH) : idx / max(1, row_nb(kind, p.u_n, p.CH));
+    int r, sub = 0, fin = 0;
+    if (isA) {
+      r = p.uniform ? idx / una : p.a_row[idx];
+    } else if (p.uniform) {
+      uniform_b_item(idx, p.B, unc, ufin, p.fin_delay, &r, &sub, &fin);
     } else {
-      r = isA ? p.a_row[idx] : p.b_row[idx];
+      const int32_t v = p.b_row[idx];
+      r = v & 0x7FFFFFFF;
+      fin = (v >> 31) & 1;
     }
     const RowCtx rc = load_row<VT, SCALE>(p, r);
-    int fin = -1;
+    if (!p.uniform && !isA && !fin) sub = idx - rc.b0;
+    const bool streaming = isA ? (rc.kind == kKindAll || rc.kind == kKindGridRadix)
+                               : (!fin && (rc.kind == kKindGridPref || rc.kind == kKindGridRadix));
+    if (!streaming) e.do_release();
     if (isA) {
       switch (rc.kind) {
-        case kKindSmem: e.smem_row(r, rc); break;
-        case kKindCta: e.cta_row(r, rc); break;
-        case kKindAll:
-          if (e.all_item(r, rc, idx - rc.a0)) fin = r;
+        case kKindSmem:
+          if (threadIdx.x == 0) m->ring_dirty = 1;
+          e.smem_row(r, rc);
           break;
-        case kKindGridPref: e.sample_item(r, rc); break;
+        case kKindCta:
+          if (threadIdx.x == 0) m->ring_dirty = 1;
+          e.cta_row(r, rc);
+          break;
+        case kKindAll: e.all_item(r, rc, idx - rc.a0); break;
+        case kKindGridPref:
+          if (threadIdx.x == 0) m->ring_dirty = 1;
+          e.sample_item(r, rc);
+          break;
         case kKindGridRadix: e.h_item(r, rc, idx - rc.a0); break;
         default: break;
       }
-    } else {
-      if (rc.kind == kKindGridPref) {
-        if (e.pf_item(r, rc, idx - rc.b0)) fin = r;
-      } else if (rc.kind == kKindGridRadix) {
-        if (e.f_item(r, rc, idx - rc.b0)) fin = r;
-      }
+    } else if (fin) {
+      if (threadIdx.x == 0) m->ring_dirty = 1;
+      e.fin_item(r, rc);
+    } else if (rc.kind == kKindGridPref) {
+      e.pf_item(r, rc, sub);
+    } else if (rc.kind == kKindGridRadix) {
+      e.f_item(r, rc, sub);
     }
-    if (pending >= 0) {
-      e.finish_row(pending);
-      pending = -1;
-    }
-    pending = fin;
     __syncthreads();
-    if (threadIdx.x == 0) m->next_q = prefetch ? (int)nq : (int)atomicAdd(&p.hdr->qhead, 1u);
+    if (threadIdx.x == 0) m->next_q = (int)nq;
     __syncthreads();
     q = m->next_q;
   }
+  e.pending_rel = m->rel_row;
+  e.do_release();
   e.phase_b();
 }
 

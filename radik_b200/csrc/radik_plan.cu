@@ -19,7 +19,7 @@ __device__ int64_t block_excl_scan64(int64_t v, int64_t* scan, int64_t* total) {
   if (lane == 31) scan[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    int64_t w = scan[lane];
+    int64_t w = lane < kWarps ? scan[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int64_t y = __shfl_up_sync(kFull, w, o);
@@ -34,10 +34,15 @@ __device__ int64_t block_excl_scan64(int64_t v, int64_t* scan, int64_t* total) {
   return base + x - v;
 }
 
+// Plans a batch: per row its kind, A items (a0) and B block (b0), candidate
+// and sort-scratch regions, histogram-ring ordinal; the A and B item -> row
+// maps (a B entry with the top bit set is the row's FIN item, placed at the
+// end of the block of row r + D, or in a tail after the last block); and
+// the claim-order lag that keeps every B item after its row's A items.
 __global__ void __launch_bounds__(kThreads, 1)
-    plan_kernel(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* a_row, int32_t* b_row,
-                Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total, int64_t sort_cap_total,
-                int grid) {
+    plan_kernel(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
+                int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
+                int64_t sort_cap_total, int grid) {
   __shared__ int64_t scan[32];
   __shared__ int64_t run[5];
   __shared__ long long maxlag;
@@ -49,17 +54,21 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
   const bool sorted = (flags & kFlagSorted) != 0;
+  auto kind_of = [&](int r) {
+    const RowDesc d = desc[r];
+    return row_kind(d.n < 0 ? 0 : d.n, d.k);
+  };
   for (int base = 0; base < B; base += kThreads) {
     const int r = base + threadIdx.x;
-    int64_t na = 0, nb = 0, cand = 0, sortn = 0, hist = 0;
+    int64_t na = 0, blk = 0, cand = 0, sortn = 0, hist = 0;
     RowDesc d{0, 0, 0, 0};
     int kind = kKindEmpty;
     if (r < B) {
       d = desc[r];
       if (d.n < 0) d.n = 0;
       kind = row_kind(d.n, d.k);
-      na = row_na(kind, d.n, CH);
-      nb = row_nb(kind, d.n, CH);
+      na = row_na(kind, d.n, CH, CHR);
+      blk = row_nbc(kind, d.n, CH, CHR) + ((r >= D) ? row_fin(kind_of(r - D)) : 0);
       cand = row_cand_cap(kind, d.n);
       hist = row_uses_hist(kind);
       if (kind == kKindGridRadix) has_radix = 1;
@@ -68,7 +77,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     int64_t t0, t1, t2, t3, t4;
     const int64_t e0 = block_excl_scan64(na, scan, &t0);
-    const int64_t e1 = block_excl_scan64(nb, scan, &t1);
+    const int64_t e1 = block_excl_scan64(blk, scan, &t1);
     const int64_t e2 = block_excl_scan64(cand, scan, &t2);
     const int64_t e3 = block_excl_scan64(sortn, scan, &t3);
     const int64_t e4 = block_excl_scan64(hist, scan, &t4);
@@ -86,8 +95,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       pl.slot_use = hist ? (int32_t)(run[4] + e4) : -1;
       pl.pad0 = pl.pad1 = 0;
       plans[r] = pl;
-      // B items of this row must come after its A items in the claim order.
-      if (nb > 0) atomicMax(&maxlag, (long long)(pl.a0 + na - pl.b0));
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -99,29 +106,55 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncthreads();
   }
-  const bool ok = run[0] <= na_cap && run[1] <= nb_cap && run[2] <= cand_cap_total && run[3] <= sort_cap_total &&
-                  run[0] + run[1] < (1ll << 30);
+  // FIN items of the last min(D, B) rows form the tail of the B sequence
+  const int Dd = D < B ? D : B;
+  int64_t tail = 0;
+  for (int r = B - Dd; r < B; ++r) tail += row_fin(kind_of(r)) ? 1 : 0;  // same value in every thread
+  const int64_t nb_total = run[1] + tail;
+  const bool ok = run[0] <= na_cap && nb_total <= nb_cap && run[2] <= cand_cap_total && run[3] <= sort_cap_total &&
+                  run[0] + nb_total < (1ll << 30);
   if (threadIdx.x == 0) {
     hdr->na = (int32_t)run[0];
-    hdr->nb = (int32_t)run[1];
+    hdr->nb = (int32_t)nb_total;
     hdr->cand_total = run[2];
     hdr->sort_total = run[3];
-    // see lag_floor() on the host side
-    const long long floor_ = has_radix ? 2LL * grid : (long long)max(2, grid / 4);
-    hdr->lag = (int32_t)max(floor_, maxlag + 1);
     hdr->plan_error = ok ? 0 : 1;
     if (!ok) atomicOr(&hdr->status, kStatusCapacity);
   }
   if (!ok) return;
   __syncthreads();
-  // one warp per row fills the item -> row maps
+  // item -> row maps, one warp per row; FIN positions and the lag
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t tail_base = run[1];
   for (int r = warp; r < B; r += kWarps) {
     const RowPlan& pl = plans[r];
     const int kind = row_kind(pl.n, pl.k);
-    const int32_t na = row_na(kind, pl.n, CH), nb = row_nb(kind, pl.n, CH);
+    const int32_t na = row_na(kind, pl.n, CH, CHR), nbc = row_nbc(kind, pl.n, CH, CHR);
     for (int c = lane; c < na; c += 32) a_row[pl.a0 + c] = r;
-    for (int c = lane; c < nb; c += 32) b_row[pl.b0 + c] = r;
+    for (int c = lane; c < nbc; c += 32) b_row[pl.b0 + c] = r;
+    if (lane == 0) {
+      int64_t first_b = nbc > 0 ? pl.b0 : -1;
+      if (row_fin(kind)) {
+        int64_t pos;
+        if (r + D < B) {
+          const RowPlan& q = plans[r + D];
+          pos = q.b0 + row_nbc(row_kind(q.n, q.k), q.n, CH, CHR);
+        } else {
+          int64_t t = 0;  // FIN items of rows B-Dd .. r-1
+          for (int x = B - Dd; x < r; ++x) t += row_fin(kind_of(x)) ? 1 : 0;
+          pos = tail_base + t;
+        }
+        b_row[pos] = (int32_t)((uint32_t)r | 0x80000000u);
+        if (first_b < 0) first_b = pos;
+      }
+      if (first_b >= 0) atomicMax(&maxlag, (long long)(pl.a0 + na - first_b));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // see lag_floor() on the host side
+    const long long floor_ = has_radix ? 2LL * grid : (long long)max(2, grid / 4);
+    hdr->lag = (int32_t)max(floor_, maxlag + 1);
   }
 }
 
@@ -136,10 +169,10 @@ cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream
   }
 }
 
-cudaError_t launch_plan(const RowDesc* desc, int B, int CH, uint32_t flags, RowPlan* plans, int32_t* a_row,
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
                         int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
                         int64_t sort_cap_total, int grid, cudaStream_t stream) {
-  dev::plan_kernel<<<1, kThreads, 0, stream>>>(desc, B, CH, flags, plans, a_row, b_row, hdr, na_cap, nb_cap,
+  dev::plan_kernel<<<1, kThreads, 0, stream>>>(desc, B, CH, CHR, D, flags, plans, a_row, b_row, hdr, na_cap, nb_cap,
                                                cand_cap_total, sort_cap_total, grid);
   return cudaGetLastError();
 }
@@ -158,7 +191,7 @@ cudaError_t engine_max_grid(int dtype, uint32_t flags, int* grid) {
     default: e = occupancy_bf16(flags, &per); break;
   }
   if (e != cudaSuccess) return e;
-  *grid = per > 0 ? sms : 0;
+  *grid = sms * (per < kCtasPerSM ? per : kCtasPerSM);
   return cudaSuccess;
 }
 

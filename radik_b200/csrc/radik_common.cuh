@@ -33,8 +33,8 @@ enum : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 // ----------------------------------------------------------------------------
 // Engine geometry
 // ----------------------------------------------------------------------------
-constexpr int kThreads = 512;            // two CTAs per SM, 16 warps each
-constexpr int kCtasPerSM = 2;
+constexpr int kThreads = 1024;           // one CTA per SM: 24 consumer, 7 side, 1 producer warp
+constexpr int kCtasPerSM = 1;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCapSB = 10240;            // candidates a finisher resolves in smem (80 KB)
 constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
@@ -47,7 +47,7 @@ constexpr int kSampleMax = 16384;        // sampled keys per row (64 KB smem)
 constexpr int kSampleMin = 1024;
 constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
 constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)
-constexpr int kSmemBytes = 100 * 1024;   // dynamic smem per CTA (two fit an SM)
+constexpr int kSmemBytes = 224 * 1024;   // dynamic smem per CTA
 constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scratch
 
 // Row kinds (a function of n and k only).

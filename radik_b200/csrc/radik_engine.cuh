@@ -191,33 +191,37 @@ __device__ __forceinline__ uint32_t out_key_inv(uint32_t k, bool ascend) {
 // ----------------------------------------------------------------------------
 // Shared-memory scratch at the tail of the dynamic allocation
 // ----------------------------------------------------------------------------
-// Streaming ring: kStages slots of kStageBytes at the start of smem, filled by
-// bulk copies; per-warp staging buffers behind it.
-constexpr int kStages = 5;
-constexpr int kStageBytes = 16384;
-constexpr int kStageVecs = kStageBytes / 16;
-constexpr int kRingBytes = kStages * kStageBytes;       // 80 KB
+// Shared memory of a CTA (kSmemBytes):
+//   ring           kStages x kStageBytes, filled by the producer's bulk copies
+//   consumer area  per-warp staging buffers / first-digit histogram
+//   side area      sampled keys, candidate entries, sort and resolve scratch
+//   control        per-team scratch (Misc), ring and queue mbarriers
+constexpr int kStages = 4;
+constexpr int kStageVecs = 24 * 32 * 2;                 // two 16-byte vectors per consumer thread
+constexpr int kStageBytes = kStageVecs * 16;            // 24 KB
+constexpr int kRingBytes = kStages * kStageBytes;       // 96 KB
+constexpr int kConsAreaOff = kRingBytes;
+constexpr int kConsAreaBytes = 24 * 1024;
+constexpr int kSideAreaOff = kConsAreaOff + kConsAreaBytes;
+constexpr int kSideAreaBytes = 96 * 1024;
+constexpr int kCtrlOff = kSideAreaOff + kSideAreaBytes;  // 216 KB
 constexpr int kSinkCand = 96;                           // filter items: candidate entries per warp
 constexpr int kSinkOut = 32;                            // filter / copy items: output entries per warp
 constexpr int kSinkPf = 128;                            // pre-filter items: candidate entries per warp
-constexpr int kSinkCandOff = kRingBytes;                // kWarps x kSinkCand x 8 B (12 KB)
-constexpr int kSinkOutOff = kSinkCandOff + kWarps * kSinkCand * 8;  // kWarps x kSinkOut x 8 B (4 KB)
-constexpr int kSinkPfOff = kRingBytes;                  // kWarps x kSinkPf x 8 B (16 KB)
-constexpr int kHistOff = kRingBytes;                    // first-digit histogram (<= 16 KB)
+// offsets inside an area
+constexpr int kHistOff = 0;                             // first-digit histogram (<= 16 KB)
 constexpr int kResolveHistOff = kCapSB * 8;             // 4096-bin histogram behind a finisher's entries
 constexpr int kSmemRowHistOff = kSmemRowCap * 4;        // behind an smem row's values
 constexpr int kSampleHistOff = kSampleMax * 4;          // behind the sampled keys
-static_assert(kSinkPfOff + kWarps * kSinkPf * 8 <= kSmemBytes - kMiscBytes, "pre-filter smem");
-static_assert(kSinkOutOff + kWarps * kSinkOut * 8 <= kSmemBytes - kMiscBytes, "filter smem");
-static_assert(kHistOff + (4 << kMaxD1) <= kSmemBytes - kMiscBytes, "histogram smem");
-static_assert(kResolveHistOff + 16384 <= kSmemBytes - kMiscBytes, "finisher smem");
-static_assert(kSmemRowHistOff + kCapSort * 8 <= kSmemBytes - kMiscBytes, "smem-row sort area");
-static_assert(kSampleHistOff + 16384 <= kSmemBytes - kMiscBytes, "sample smem");
-static_assert(kCapSort * 8 <= kSmemBytes - kMiscBytes, "sort smem");
+static_assert(24 * kSinkPf * 8 <= kConsAreaBytes, "pre-filter staging");
+static_assert(24 * (kSinkCand + kSinkOut) * 8 <= kConsAreaBytes, "filter staging");
+static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B staging");
+static_assert((4 << kMaxD1) <= kConsAreaBytes, "histogram");
+static_assert(kResolveHistOff + 16384 <= kSideAreaBytes, "finisher area");
+static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
+static_assert(kSampleHistOff + 16384 <= kSideAreaBytes, "sample area");
 
 struct Misc {
-  uint64_t mbar[kStages];        // ring slot filled (bulk copy bytes landed)
-  uint64_t mbar_empty[kStages];  // ring slot drained (every warp is done with it)
   uint32_t hist256[256];
   uint32_t scan[64];
   int32_t next_q;
@@ -229,27 +233,76 @@ struct Misc {
   int32_t st_mode, st_krem, st_count, st_plen;
   uint64_t st_prefix;
   int32_t st_candn;
-  int32_t pad[7];
-  uint64_t red_lo, red_hi;
-  uint64_t red_hi_w[32];
-  int32_t rel_row;     // row whose chunk counter the next iteration releases (-1: none)
+  int32_t rel_row;     // row whose chunk counter the next item releases (-1: none)
   int32_t t_row;       // row of the cached pre-filter threshold (-1: none)
   uint32_t t_val;      // the cached threshold
-  int32_t ring_dirty;  // the ring's smem was written by a non-streaming item
+  int32_t pad[4];
+  uint64_t red_lo, red_hi;
+  uint64_t red_hi_w[32];
   int32_t pbtab[200];  // phase-B row table (row ids, chunk counts, prefix)
 };
-static_assert(sizeof(Misc) <= kMiscBytes, "Misc too large");
+static_assert(sizeof(Misc) <= 3072, "Misc too large");
 
-__device__ __forceinline__ Misc* misc_of(uint8_t* smem) {
-  return reinterpret_cast<Misc*>(smem + (kSmemBytes - kMiscBytes));
-}
+// A claimed work item, handed from the producer to a team.
+struct alignas(16) ItemDesc {
+  int32_t q;     // claim index, -1 = end of the queue
+  int32_t row;
+  int32_t isA;   // an A item (else a B item)
+  int32_t fin;   // a FIN item
+  int32_t sub;   // chunk index within the row
+  int32_t nst;   // bulk-copy stages of a streaming item
+  uint32_t g0;   // its first global ring stage
+  int32_t pad;
+  int64_t a, b;  // positions [a, b) of the chunk
+  int64_t va;    // first 16-byte aligned position
+  int64_t nvec;  // aligned 16-byte vectors from va
+};
+constexpr int kQ = 4;  // queue slots per team
+struct Ctrl {
+  uint64_t full[kStages];   // ring slot filled
+  uint64_t empty[kStages];  // ring slot drained by every consumer warp
+  uint64_t cq_full[kQ], cq_empty[kQ], sq_full[kQ], sq_empty[kQ];
+  ItemDesc cq[kQ], sq[kQ];
+};
+static_assert(kCtrlOff + 2 * 3072 + sizeof(Ctrl) <= kSmemBytes, "control area");
+
+__device__ __forceinline__ Misc* cons_misc(uint8_t* smem) { return reinterpret_cast<Misc*>(smem + kCtrlOff); }
+__device__ __forceinline__ Misc* side_misc(uint8_t* smem) { return reinterpret_cast<Misc*>(smem + kCtrlOff + 3072); }
+__device__ __forceinline__ Ctrl* ctrl_of(uint8_t* smem) { return reinterpret_cast<Ctrl*>(smem + kCtrlOff + 6144); }
+
+// ----------------------------------------------------------------------------
+// Thread teams.  The CTA is split by warp role: warps 0-23 stream chunks
+// (consumers), warps 24-30 do latency-bound work (samples, finishes, short
+// rows), warp 31 claims items and issues the bulk copies (producer).  Each
+// team synchronises on its own named barrier; the whole CTA on barrier 0.
+// ----------------------------------------------------------------------------
+template <int BASE, int SIZE, int BAR>
+struct TeamT {
+  static constexpr int kBase = BASE;
+  static constexpr int kSize = SIZE;
+  static constexpr int kWarps = SIZE / 32;
+  __device__ __forceinline__ static int tid() { return (int)threadIdx.x - BASE; }
+  __device__ __forceinline__ static int wid() { return ((int)threadIdx.x - BASE) >> 5; }
+  __device__ __forceinline__ static void sync() {
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(SIZE) : "memory");
+  }
+};
+constexpr int kConsWarps = 24;
+constexpr int kSideWarps = 7;
+constexpr int kProducerWarp = 31;
+using ConsTeam = TeamT<0, kConsWarps * 32, 1>;
+using SideTeam = TeamT<kConsWarps * 32, kSideWarps * 32, 2>;
+using FullTeam = TeamT<0, kThreads, 0>;
+static_assert(kConsWarps + kSideWarps + 1 == kWarps, "warp roles");
 
 // ----------------------------------------------------------------------------
 // Block primitives
 // ----------------------------------------------------------------------------
 // Exclusive scan of one value per thread; *total gets the block sum.
+template <class Tm>
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* scan, uint32_t* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = Tm::wid();
   uint32_t x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -257,9 +310,9 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* scan, 
     if (lane >= o) x += y;
   }
   if (lane == 31) scan[warp] = x;
-  __syncthreads();
+  Tm::sync();
   if (warp == 0) {
-    uint32_t w = lane < kWarps ? scan[lane] : 0u;
+    uint32_t w = lane < Tm::kWarps ? scan[lane] : 0u;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(kFull, w, o);
@@ -267,20 +320,20 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* scan, 
     }
     scan[lane] = w;
   }
-  __syncthreads();
+  Tm::sync();
   const uint32_t base = warp ? scan[warp - 1] : 0u;
-  if (total) *total = scan[kWarps - 1];
-  __syncthreads();
+  if (total) *total = scan[Tm::kWarps - 1];
+  Tm::sync();
   return base + x - v;
 }
 
 // Finds the bin b of h[0..NB) with cum(<b) < krem <= cum(<=b).
 // Result in m->sel_*; m->sel_found = 0 if the bins hold fewer than krem.
-template <bool GLOBAL>
+template <class Tm, bool GLOBAL>
 __device__ void block_select(const uint32_t* h, int NB, uint32_t krem, Misc* m) {
-  if (threadIdx.x == 0) m->sel_found = 0;
-  const int per = (NB + kThreads - 1) / kThreads;
-  const int lo = threadIdx.x * per;
+  if (Tm::tid() == 0) m->sel_found = 0;
+  const int per = (NB + Tm::kSize - 1) / Tm::kSize;
+  const int lo = Tm::tid() * per;
   const int hi = min(NB, lo + per);
   uint32_t s = 0;
   if ((per & 3) == 0) {
@@ -293,7 +346,7 @@ __device__ void block_select(const uint32_t* h, int NB, uint32_t krem, Misc* m) 
   } else {
     for (int i = lo; i < hi; ++i) s += GLOBAL ? ld_cg_u32(h + i) : h[i];
   }
-  const uint32_t ex = block_excl_scan(s, m->scan, nullptr);
+  const uint32_t ex = block_excl_scan<Tm>(s, m->scan, nullptr);
   if (lo < hi && ex < krem && krem <= ex + s) {
     uint32_t run = ex;
     for (int i = lo; i < hi; ++i) {
@@ -308,7 +361,7 @@ __device__ void block_select(const uint32_t* h, int NB, uint32_t krem, Misc* m) 
       run += c;
     }
   }
-  __syncthreads();
+  Tm::sync();
 }
 
 // Shared-memory histogram increment, aggregated: the bin of the first valid
@@ -342,10 +395,11 @@ __device__ __forceinline__ void hist_add(uint32_t* hist, uint32_t bin, bool vali
 }
 
 // Bitonic sort of n (power of two, >= 2) uint64 keys in shared memory.
+template <class Tm>
 __device__ inline void block_bitonic_sort(uint64_t* s, int n) {
   for (int size = 2; size <= n; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = threadIdx.x; i < (n >> 1); i += kThreads) {
+      for (int i = Tm::tid(); i < (n >> 1); i += Tm::kSize) {
         const int lo = 2 * i - (i & (stride - 1));
         const int hi = lo + stride;
         const bool up = (lo & size) == 0;
@@ -355,7 +409,7 @@ __device__ inline void block_bitonic_sort(uint64_t* s, int n) {
           s[hi] = a;
         }
       }
-      __syncthreads();
+      Tm::sync();
     }
   }
 }
@@ -428,7 +482,7 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
 // Both callbacks are called by every thread the same number of times (warp
 // collectives are allowed inside).
 // ----------------------------------------------------------------------------
-template <int ES, int U, typename FE, typename FV>
+template <class Tm, int ES, int U, typename FE, typename FV>
 __device__ __forceinline__ void for_range_v(const void* base, int64_t in_off, int64_t a, int64_t b, FE&& fe,
                                             FV&& fv) {
   constexpr int VEC = 16 / ES;
@@ -442,7 +496,7 @@ __device__ __forceinline__ void for_range_v(const void* base, int64_t in_off, in
   const int64_t vb = va + nvec * VEC;
   const int64_t tail = b - vb;
   if (head > 0 || tail > 0) {
-    const int t = threadIdx.x;
+    const int t = Tm::tid();
     const bool vh = t < head;
     const bool vt = t < tail;
     uint32_t bh = 0, bt = 0;
@@ -454,19 +508,19 @@ __device__ __forceinline__ void for_range_v(const void* base, int64_t in_off, in
     if (tail > 0) fe(bt, vb + t, vt);
   }
   const uint4* vp = reinterpret_cast<const uint4*>(row + va * ES);
-  const int64_t step = (int64_t)kThreads * U;
+  const int64_t step = (int64_t)Tm::kSize * U;
   const int64_t iters = (nvec + step - 1) / step;
-  int64_t v0 = threadIdx.x;
+  int64_t v0 = Tm::tid();
   for (int64_t it = 0; it < iters; ++it, v0 += step) {
     uint4 x[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int64_t v = v0 + (int64_t)u * kThreads;
+      const int64_t v = v0 + (int64_t)u * Tm::kSize;
       x[u] = v < nvec ? ld_stream16(vp + v) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int64_t v = v0 + (int64_t)u * kThreads;
+      const int64_t v = v0 + (int64_t)u * Tm::kSize;
       fv(x[u], va + v * VEC, v < nvec);
     }
   }
@@ -569,6 +623,7 @@ __device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint
 // Shared-memory selection
 // ----------------------------------------------------------------------------
 // Block-wide min of lo and max of hi over all threads (pass ~0 / 0 to abstain).
+template <class Tm>
 __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t* mn, uint64_t* mx, Misc* m) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -576,15 +631,15 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
     hi = max(hi, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)hi, o));
   }
   uint64_t* red = reinterpret_cast<uint64_t*>(m->scan);  // 64 x u32 = 32 x u64
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
+  const int warp = Tm::wid(), lane = threadIdx.x & 31;
+  Tm::sync();
   if (lane == 0) {
     red[warp] = lo;
     m->red_hi_w[warp] = hi;
   }
-  __syncthreads();
+  Tm::sync();
   if (warp == 0) {
-    uint64_t a = lane < kWarps ? red[lane] : ~0ull, b = lane < kWarps ? m->red_hi_w[lane] : 0ull;
+    uint64_t a = lane < Tm::kWarps ? red[lane] : ~0ull, b = lane < Tm::kWarps ? m->red_hi_w[lane] : 0ull;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       a = min(a, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)a, o));
@@ -595,10 +650,10 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
       m->red_hi = b;
     }
   }
-  __syncthreads();
+  Tm::sync();
   *mn = m->red_lo;
   *mx = m->red_hi;
-  __syncthreads();
+  Tm::sync();
 }
 
 // Threshold key of a sample: the r-th smallest (1-based) of cnt KB-bit keys
@@ -606,16 +661,16 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
 // skipped (min/max reduction); then at most two 12-bit digits refine it.
 // When bits remain after that, the upper edge of the r-th key's bin is
 // returned (at least r keys are <= it).  hist: 4096 counters of smem.
-template <int KB>
+template <class Tm, int KB>
 __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r, uint32_t* hist, Misc* m,
                                            int32_t* status) {
   uint64_t lo = ~0ull, hi = 0;
-  for (int i = threadIdx.x; i < cnt; i += kThreads) {
+  for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
     lo = min(lo, (uint64_t)keys[i]);
     hi = max(hi, (uint64_t)keys[i]);
   }
   uint64_t mn, mx;
-  block_minmax(lo, hi, &mn, &mx, m);
+  block_minmax<Tm>(lo, hi, &mn, &mx, m);
   if (mn >= mx) return (uint32_t)mn;
   int plen = __clzll((long long)(mn ^ mx)) - (64 - KB);  // shared leading bits
   uint32_t prefix = plen > 0 ? (uint32_t)(mn >> (KB - plen)) : 0u;
@@ -623,24 +678,24 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
   for (int level = 0; level < 2 && plen < KB; ++level) {
     const int D = min(12, KB - plen);
     const int NB = 1 << D;
-    for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
-    __syncthreads();
+    for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+    Tm::sync();
     const int sd = KB - plen - D;
-    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
       const uint32_t k = keys[i];
       const bool match = plen == 0 || (k >> (KB - plen)) == prefix;
       if (match) atomicAdd(&hist[(k >> sd) & (uint32_t)(NB - 1)], 1u);
     }
-    __syncthreads();
-    block_select<false>(hist, NB, krem, m);
+    Tm::sync();
+    block_select<Tm, false>(hist, NB, krem, m);
     if (!m->sel_found) {
-      if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
+      if (Tm::tid() == 0) atomicOr(status, kStatusSelect);
       return (uint32_t)(((uint64_t)1 << KB) - 1);
     }
     prefix = (prefix << D) | m->sel_bin;
     plen += D;
     krem -= m->sel_cum;
-    __syncthreads();
+    Tm::sync();
   }
   if (plen >= KB) return prefix;
   return (uint32_t)(((uint64_t)prefix << (KB - plen)) | (((uint64_t)1 << (KB - plen)) - 1));
@@ -651,14 +706,14 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
 // equals krem: first past the bits all entries share (min/max reduction),
 // then with 12-bit digits (hist: 4096 counters of smem).  On return the
 // selected entries are those whose composite prefix is <= prefix.
-template <int VT, bool SCALE, typename G>
+template <class Tm, int VT, bool SCALE, typename G>
 __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix, int& plen, int& krem, int count,
                              uint32_t* hist, Misc* m, int32_t* status) {
   using K = KT<VT, SCALE>;
   const int W = K::KB + rc.IB;
   if (count != krem && cnt > 0) {
     uint64_t lo = ~0ull, hi = 0;
-    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
       uint32_t bits;
       int64_t pos;
       get(i, bits, pos);
@@ -669,7 +724,7 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
       }
     }
     uint64_t mn, mx;
-    block_minmax(lo, hi, &mn, &mx, m);
+    block_minmax<Tm>(lo, hi, &mn, &mx, m);
     if (mn != ~0ull) {
       const int common = (mn == mx) ? W : (__clzll((long long)(mn ^ mx)) - (64 - W));
       if (common > plen) {
@@ -680,47 +735,47 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
   }
   while (count != krem) {
     if (plen >= W || count < krem) {
-      if (threadIdx.x == 0) atomicOr(status, kStatusLevels);
+      if (Tm::tid() == 0) atomicOr(status, kStatusLevels);
       break;
     }
     const int D = min(12, W - plen);
     const int NB = 1 << D;
-    for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
-    __syncthreads();
+    for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+    Tm::sync();
     const int sh = W - plen;
     const int sd = W - plen - D;
     const uint32_t dm = (uint32_t)NB - 1u;
-    for (int i = threadIdx.x; i < cnt; i += kThreads) {
+    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
       uint32_t bits;
       int64_t pos;
       get(i, bits, pos);
       const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
       if (shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
     }
-    __syncthreads();
-    block_select<false>(hist, NB, (uint32_t)krem, m);
+    Tm::sync();
+    block_select<Tm, false>(hist, NB, (uint32_t)krem, m);
     if (!m->sel_found) {
-      if (threadIdx.x == 0) atomicOr(status, kStatusSelect);
+      if (Tm::tid() == 0) atomicOr(status, kStatusSelect);
       break;
     }
     prefix = (prefix << D) | m->sel_bin;
     plen += D;
     krem -= (int)m->sel_cum;
     count = (int)m->sel_cnt;
-    __syncthreads();
+    Tm::sync();
   }
 }
 
 // Emits the entries selected by (prefix, plen) to the row's output, in entry
 // order, reserving the slots with one atomic on the row's out_count.
-template <int VT, bool SCALE, typename G>
+template <class Tm, int VT, bool SCALE, typename G>
 __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& rc, uint64_t prefix, int plen,
                           RowState* rs, Misc* m) {
   using K = KT<VT, SCALE>;
   const int W = K::KB + rc.IB;
   const int sh = W - plen;
-  const int per = (cnt + kThreads - 1) / kThreads;
-  const int lo = min(cnt, (int)threadIdx.x * per);
+  const int per = (cnt + Tm::kSize - 1) / Tm::kSize;
+  const int lo = min(cnt, Tm::tid() * per);
   const int hi = min(cnt, lo + per);
   uint32_t mine = 0;
   for (int i = lo; i < hi; ++i) {
@@ -731,9 +786,9 @@ __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& r
     mine += shr64(c, sh) <= prefix;
   }
   uint32_t total;
-  const uint32_t ex = block_excl_scan(mine, m->scan, &total);
-  if (threadIdx.x == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
-  __syncthreads();
+  const uint32_t ex = block_excl_scan<Tm>(mine, m->scan, &total);
+  if (Tm::tid() == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
+  Tm::sync();
   int64_t slot = (int64_t)m->counter + ex;
   for (int i = lo; i < hi; ++i) {
     uint32_t bits;
@@ -745,13 +800,13 @@ __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& r
       ++slot;
     }
   }
-  __syncthreads();
+  Tm::sync();
 }
 
 // ----------------------------------------------------------------------------
 // Row post-processing: sort, index mapping, idle fill
 // ----------------------------------------------------------------------------
-template <int VT, bool SCALE>
+template <class Tm, int VT, bool SCALE>
 __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* smem, Misc* m) {
   const int64_t kk = min((int64_t)rc.n, (int64_t)rc.k);
   const bool idx64 = (p.flags & kFlagIdx64) != 0;
@@ -759,7 +814,7 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
   const bool sorting = (p.flags & kFlagSorted) && kk > 1;
   if (!sorting && !withidx && kk == rc.k) return;  // unsorted, positions, no idle slots: nothing to do
   __threadfence();
-  __syncthreads();
+  Tm::sync();
   auto load_pos = [&](int64_t i) -> int64_t {
     return idx64 ? (int64_t)__ldcg(reinterpret_cast<const long long*>(p.idx_out) + rc.out_off + i)
                  : (int64_t)__ldcg(static_cast<const int32_t*>(p.idx_out) + rc.out_off + i);
@@ -779,14 +834,14 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
       uint64_t* s = reinterpret_cast<uint64_t*>(smem);
       int np = 2;
       while (np < kk) np <<= 1;
-      for (int i = threadIdx.x; i < np; i += kThreads) {
+      for (int i = Tm::tid(); i < np; i += Tm::kSize) {
         uint64_t v = ~0ull;
         if (i < kk) v = ((uint64_t)out_key<VT>(load_bits(i), ascend) << 32) | (uint64_t)(uint32_t)load_pos(i);
         s[i] = v;
       }
-      __syncthreads();
-      block_bitonic_sort(s, np);
-      for (int i = threadIdx.x; i < kk; i += kThreads) {
+      Tm::sync();
+      block_bitonic_sort<Tm>(s, np);
+      for (int i = Tm::tid(); i < kk; i += Tm::kSize) {
         const uint64_t v = s[i];
         const int64_t pos = (int64_t)(uint32_t)v;
         write_out<VT>(p, rc.out_off + i, out_key_inv<VT>((uint32_t)(v >> 32), ascend), map_idx(pos));
@@ -800,23 +855,23 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
       uint64_t* s = reinterpret_cast<uint64_t*>(smem);
       for (int64_t r0 = 0; r0 < kk; r0 += kCapSort) {
         const int len = (int)min((int64_t)kCapSort, kk - r0);
-        for (int i = threadIdx.x; i < kCapSort; i += kThreads) {
+        for (int i = Tm::tid(); i < kCapSort; i += Tm::kSize) {
           uint64_t v = ~0ull;
           if (i < len)
             v = ((uint64_t)out_key<VT>(load_bits(r0 + i), ascend) << 32) | (uint64_t)(uint32_t)load_pos(r0 + i);
           s[i] = v;
         }
-        __syncthreads();
-        block_bitonic_sort(s, kCapSort);
-        for (int i = threadIdx.x; i < len; i += kThreads) a[r0 + i] = s[i];
-        __syncthreads();
+        Tm::sync();
+        block_bitonic_sort<Tm>(s, kCapSort);
+        for (int i = Tm::tid(); i < len; i += Tm::kSize) a[r0 + i] = s[i];
+        Tm::sync();
       }
       for (int64_t run = kCapSort; run < kk; run <<= 1) {
         for (int64_t m0 = 0; m0 < kk; m0 += 2 * run) {
           const int64_t l0 = m0, l1 = min(kk, m0 + run), r1 = min(kk, m0 + 2 * run);
           const int64_t tot = r1 - l0;
-          const int64_t per = (tot + kThreads - 1) / kThreads;
-          const int64_t d0 = min(tot, (int64_t)threadIdx.x * per), d1 = min(tot, d0 + per);
+          const int64_t per = (tot + Tm::kSize - 1) / Tm::kSize;
+          const int64_t d0 = min(tot, (int64_t)Tm::tid() * per), d1 = min(tot, d0 + per);
           auto split = [&](int64_t d) -> int64_t {  // elements taken from the left run
             int64_t lo = max((int64_t)0, d - (r1 - l1)), hi = min(d, l1 - l0);
             while (lo < hi) {
@@ -838,34 +893,35 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
             }
           }
         }
-        __syncthreads();
+        Tm::sync();
         uint64_t* t = a;
         a = b;
         b = t;
       }
-      for (int64_t i = threadIdx.x; i < kk; i += kThreads) {
+      for (int64_t i = Tm::tid(); i < kk; i += Tm::kSize) {
         const uint64_t v = ld_cg_u64(a + i);
         write_out<VT>(p, rc.out_off + i, out_key_inv<VT>((uint32_t)(v >> 32), ascend), map_idx((int64_t)(uint32_t)v));
       }
     }
   } else if (withidx) {
-    for (int64_t i = threadIdx.x; i < kk; i += kThreads) {
+    for (int64_t i = Tm::tid(); i < kk; i += Tm::kSize) {
       const int64_t pos = load_pos(i);
       const int64_t mapped = map_idx(pos);
       if (idx64) static_cast<int64_t*>(p.idx_out)[rc.out_off + i] = mapped;
       else static_cast<int32_t*>(p.idx_out)[rc.out_off + i] = (int32_t)mapped;
     }
   }
-  for (int64_t i = kk + threadIdx.x; i < rc.k; i += kThreads) write_out<VT>(p, rc.out_off + i, 0u, -1);
-  __syncthreads();
+  for (int64_t i = kk + Tm::tid(); i < rc.k; i += Tm::kSize) write_out<VT>(p, rc.out_off + i, 0u, -1);
+  Tm::sync();
 }
 
 // ----------------------------------------------------------------------------
 // Grid barrier (cooperative launch: all CTAs are resident).  Bounded.
 // ----------------------------------------------------------------------------
+template <class Tm>
 __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  Tm::sync();
+  if (Tm::tid() == 0) {
     const uint32_t gen = ld_acquire(&h->bar_gen);
     __threadfence();
     const uint32_t arrived = atomicAdd(&h->bar_count, 1u) + 1u;
@@ -885,7 +941,7 @@ __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
     }
     __threadfence();
   }
-  __syncthreads();
+  Tm::sync();
 }
 
 // ----------------------------------------------------------------------------
@@ -899,19 +955,31 @@ struct Engine {
   static constexpr int U = 4;
 
   const EngineParams& p;
-  uint8_t* smem;
-  Misc* m;
-  uint32_t gstage = 0;  // ring stages consumed so far by this CTA (uniform)
-  int pending_rel = -1; // row whose chunk counter is still to be released (uniform)
+  uint8_t* base;  // the CTA's shared memory
+  uint8_t* smem;  // this team's area (consumer or side)
+  Misc* m;        // this team's scratch
+  Ctrl* ctl;
+  int pending_rel = -1;  // consumer team: row whose chunk counter is still to be released
+
+  __device__ Engine(const EngineParams& p_, uint8_t* b, uint8_t* area, Misc* m_)
+      : p(p_), base(b), smem(area), m(m_), ctl(ctrl_of(b)) {}
+
+  template <class Tm>
+  __device__ uint64_t* cand_sink() const {
+    return reinterpret_cast<uint64_t*>(smem) + Tm::wid() * kSinkCand;
+  }
+  template <class Tm>
+  __device__ uint64_t* out_sink() const {
+    return reinterpret_cast<uint64_t*>(smem + Tm::kWarps * kSinkCand * 8) + Tm::wid() * kSinkOut;
+  }
 
   // Releases the previous chunk item's completion on its row's counter: one
-  // thread fences (the item's writes by all warps precede it through the
-  // item's closing barrier) and increments.  Called where that thread's
-  // stall overlaps other work: after a streaming item's first copies and
-  // threshold wait, or at the start of a non-streaming item.
+  // consumer thread fences (the item's writes by all consumer warps precede
+  // it through the item's closing barrier) and increments.  Called after
+  // the next item's threshold wait, so its stall overlaps the ring's data.
   __device__ void do_release() {
     if (pending_rel >= 0) {
-      if (threadIdx.x == kThreads - 32) {
+      if (ConsTeam::tid() == ConsTeam::kSize - 32) {
         __threadfence();
         atomicAdd(&p.rs[pending_rel].fticket, 1);
       }
@@ -919,108 +987,59 @@ struct Engine {
     }
   }
 
-  __device__ Engine(const EngineParams& p_, uint8_t* s) : p(p_), smem(s), m(misc_of(s)) {}
-
-  __device__ uint64_t* cand_sink(int warp) const {
-    return reinterpret_cast<uint64_t*>(smem + kSinkCandOff) + warp * kSinkCand;
-  }
-  __device__ uint64_t* out_sink(int warp) const {
-    return reinterpret_cast<uint64_t*>(smem + kSinkOutOff) + warp * kSinkOut;
-  }
-
-  // Streams positions [a, b) of a row.  The aligned middle travels through
-  // the smem ring in bulk copies of kStageBytes issued by thread 0, up to
-  // kStages in flight; every thread consumes two 16-byte vectors per stage
-  // with fv(x, pos0, ok).  A slot is refilled once all 32 warps have
-  // arrived on its "empty" barrier, so no block-wide barrier per stage.  The
-  // unaligned head and tail (< 16 bytes each) go through fe(bits, pos, ok).
-  // pre() runs once the first copies are in flight (e.g. to wait for a
-  // row's threshold).  All callbacks are called warp-uniformly.
+  // Consumes a streaming item's chunk: pre() (e.g. a threshold wait), the
+  // unaligned head and tail (< 16 bytes each) through fe(bits, pos, ok), and
+  // the aligned middle from the ring, two 16-byte vectors per consumer
+  // thread per stage, through fv(x, pos0, ok).  Each consumer warp arrives
+  // on a stage's "empty" barrier once done with it; the producer refills the
+  // slot when all have.  All callbacks are called warp-uniformly.
   template <typename PRE, typename FE, typename FV>
-  __device__ void stream_chunk(const RowCtx& rc, int64_t a, int64_t b, PRE&& pre, FE&& fe, FV&& fv) {
+  __device__ void consume_chunk(const RowCtx& rc, const ItemDesc& d, PRE&& pre, FE&& fe, FV&& fv) {
     const char* row = static_cast<const char*>(p.val_in) + rc.in_off * ES;
-    int64_t head = 0, nvec = 0, va = a;
-    if (b > a) {
-      const uintptr_t addr_a = reinterpret_cast<uintptr_t>(row + a * ES);
-      head = (int64_t)(((16u - (unsigned)(addr_a & 15u)) & 15u) / ES);
-      if (head > b - a) head = b - a;
-      va = a + head;
-      nvec = (b - va) / VEC;
-    }
-    const int64_t vb = va + nvec * VEC;
-    const int64_t tail = b > a ? b - vb : 0;
-    const uint4* src = reinterpret_cast<const uint4*>(row + va * ES);
-    const int64_t nst = (nvec + kStageVecs - 1) / kStageVecs;
-    uint4* ring = reinterpret_cast<uint4*>(smem);
-    // thread 0 only: fill the slot of stage i once its previous use drained
-    auto issue = [&](int64_t i) {
-      const uint32_t g = gstage + (uint32_t)i;
-      const uint32_t slot = g % kStages;
-      if (g >= (uint32_t)kStages) {
-        const uint32_t parity = ((g / kStages) - 1u) & 1u;
-        uint32_t it = 0;
-        while (!mbar_try_wait(&m->mbar_empty[slot], parity)) {
-          if (++it > p.spin_limit) {
-            atomicOr(&p.hdr->status, kStatusTimeout);
-            break;
-          }
-        }
-      }
-      const int64_t v0 = i * kStageVecs;
-      const uint32_t bytes = (uint32_t)min((int64_t)kStageVecs, nvec - v0) * 16u;
-      mbar_expect_tx(&m->mbar[slot], bytes);
-      bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &m->mbar[slot]);
-    };
-    if (threadIdx.x == 0 && nst > 0) {
-      // a non-streaming item may have written this smem through the generic
-      // proxy: order that before the bulk copies overwrite it
-      if (m->ring_dirty) {
-        fence_proxy_async();
-        m->ring_dirty = 0;
-      }
-      for (int64_t i = 0; i < min(nst, (int64_t)kStages); ++i) issue(i);
-    }
     pre();
     do_release();
+    const int64_t head = d.va - d.a;
+    const int64_t vb = d.va + d.nvec * VEC;
+    const int64_t tail = d.b - vb;
     if (head > 0 || tail > 0) {
-      const int t = threadIdx.x;
+      const int t = ConsTeam::tid();
       const bool vh = t < head, vt = t < tail;
       uint32_t bh = 0, bt = 0;
-      if (vh) bh = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[a + t]
-                           : (uint32_t)reinterpret_cast<const unsigned short*>(row)[a + t];
+      if (vh) bh = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[d.a + t]
+                           : (uint32_t)reinterpret_cast<const unsigned short*>(row)[d.a + t];
       if (vt) bt = ES == 4 ? reinterpret_cast<const uint32_t*>(row)[vb + t]
                            : (uint32_t)reinterpret_cast<const unsigned short*>(row)[vb + t];
-      if (head > 0) fe(bh, a + t, vh);
+      if (head > 0) fe(bh, d.a + t, vh);
       if (tail > 0) fe(bt, vb + t, vt);
     }
-    for (int64_t i = 0; i < nst; ++i) {
-      const uint32_t g = gstage + (uint32_t)i;
+    const uint4* ring = reinterpret_cast<const uint4*>(base);
+    for (int i = 0; i < d.nst; ++i) {
+      const uint32_t g = d.g0 + (uint32_t)i;
       const uint32_t slot = g % kStages;
       const uint32_t parity = (g / kStages) & 1u;
       uint32_t it = 0;
-      while (!mbar_try_wait(&m->mbar[slot], parity)) {
+      while (!mbar_try_wait(&ctl->full[slot], parity)) {
         if (++it > p.spin_limit) {
-          if (threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusTimeout);
+          if (ConsTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusTimeout);
           break;
         }
       }
-      const int64_t v0 = i * kStageVecs;
-      const int cnt = (int)min((int64_t)kStageVecs, nvec - v0);
+      const int64_t v0 = (int64_t)i * kStageVecs;
+      const int cnt = (int)min((int64_t)kStageVecs, d.nvec - v0);
       const uint4* st = ring + (size_t)slot * kStageVecs;
 #pragma unroll
-      for (int j = 0; j < kStageVecs / kThreads; ++j) {
-        const int v = j * kThreads + threadIdx.x;
+      for (int j = 0; j < kStageVecs / ConsTeam::kSize; ++j) {
+        const int v = j * ConsTeam::kSize + ConsTeam::tid();
         const bool ok = v < cnt;
         const uint4 x = ok ? st[v] : make_uint4(0, 0, 0, 0);
-        fv(x, va + (v0 + v) * VEC, ok);
+        fv(x, d.va + (v0 + v) * VEC, ok);
       }
       __syncwarp();
-      if ((threadIdx.x & 31) == 0) mbar_arrive(&m->mbar_empty[slot]);
-      if (threadIdx.x == 0 && i + kStages < nst) issue(i + kStages);
+      if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
     }
-    gstage += (uint32_t)nst;
   }
 
+  // Bounded wait by one thread until *addr >= target.
   __device__ bool spin_until_ge(const uint32_t* addr, uint32_t target) {
     for (uint32_t it = 0; it < p.spin_limit; ++it) {
       if (ld_acquire(addr) >= target) return true;
@@ -1047,22 +1066,22 @@ struct Engine {
     constexpr int SE = 32 / ES;  // elements per sector
     const int nsec = S / SE;
     const int64_t span = (int64_t)rc.n - SE;
-    for (int j = threadIdx.x; j < S; j += kThreads) {
+    for (int j = SideTeam::tid(); j < S; j += SideTeam::kSize) {
       const int i = j / SE, o = j % SE;
       const int64_t pos = (nsec > 1 ? (int64_t)i * span / (nsec - 1) : 0) + o;
       keys[j] = key_of(load_bits(rc, pos), rc);
     }
-    __syncthreads();
+    SideTeam::sync();
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
-    const uint32_t t = block_sample_threshold<K::KB>(keys, S, sample_rank(rc.n, rc.k, S), hist, m, &p.hdr->status);
-    __syncthreads();
+    const uint32_t t = block_sample_threshold<SideTeam, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), hist, m, &p.hdr->status);
+    SideTeam::sync();
     return t;
   }
 
   // ---- whole row in shared memory (n <= kSmemRowCap)
   __device__ void smem_row(int r, const RowCtx& rc) {
     uint32_t* vals = reinterpret_cast<uint32_t*>(smem);
-    for_range_v<ES, U>(
+    for_range_v<SideTeam, ES, U>(
         p.val_in, rc.in_off, 0, rc.n, [&](uint32_t bits, int64_t pos, bool ok) { if (ok) vals[pos] = bits; },
         [&](const uint4& x, int64_t pos0, bool ok) {
           if (ok) {
@@ -1070,7 +1089,7 @@ struct Engine {
             for (int e = 0; e < VEC; ++e) vals[pos0 + e] = vec_elem<ES>(x, e);
           }
         });
-    __syncthreads();
+    SideTeam::sync();
     const int kk = min(rc.n, rc.k);
     uint64_t prefix = 0;
     int plen = 0, krem = kk;
@@ -1078,10 +1097,10 @@ struct Engine {
       bits = vals[i];
       pos = i;
     };
-    smem_resolve<VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
+    smem_resolve<SideTeam, VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
                             &p.hdr->status);
-    smem_emit<VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m);
-    post_process<VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
+    smem_emit<SideTeam, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m);
+    post_process<SideTeam, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
   }
 
   // ---- one CTA, the whole row from global memory (n <= kCtaRowCap)
@@ -1106,7 +1125,7 @@ struct Engine {
       const uint32_t se = warp_reserve(to_ent ? 1u : 0u, &m->counter);
       if (to_ent && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
     };
-    for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+    for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
       for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
     });
@@ -1123,28 +1142,28 @@ struct Engine {
     if ((int64_t)rc.k * kPrefRatio <= rc.n) {
       // pre-filter inside the CTA
       const uint32_t T = sample_threshold(rc);
-      if (threadIdx.x == 0) m->counter = 0;
-      __syncthreads();
+      if (SideTeam::tid() == 0) m->counter = 0;
+      SideTeam::sync();
       auto one = [&](uint32_t bits, int64_t pos, bool ok) {
         const bool hit = ok && key_of(bits, rc) <= T;
         if (!__any_sync(kFull, hit)) return;
         const uint32_t se = warp_reserve(hit ? 1u : 0u, &m->counter);
         if (hit && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
       };
-      for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
       });
-      __syncthreads();
+      SideTeam::sync();
       const int c = (int)m->counter;
-      __syncthreads();
+      SideTeam::sync();
       if (c >= rc.k && c <= kCapSB) {
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+        smem_resolve<SideTeam, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                                 &p.hdr->status);
-        smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
-        post_process<VT, SCALE>(p, rc, smem, m);
+        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
         return;
       }
       // threshold missed: radix levels below
@@ -1156,55 +1175,54 @@ struct Engine {
     for (int guard = 0; guard < 16 && count != krem && count > kCapSB; ++guard) {
       const int D = min(12, W - plen);
       const int NB = 1 << D;
-      for (int i = threadIdx.x; i < NB; i += kThreads) hist[i] = 0;
-      __syncthreads();
+      for (int i = SideTeam::tid(); i < NB; i += SideTeam::kSize) hist[i] = 0;
+      SideTeam::sync();
       const int sh = W - plen, sd = W - plen - D;
       const uint32_t dm = (uint32_t)NB - 1u;
       auto one = [&](uint32_t bits, int64_t pos, bool ok) {
         const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
         hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
       };
-      for_range_v<ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
       });
-      __syncthreads();
-      block_select<false>(hist, NB, (uint32_t)krem, m);
+      SideTeam::sync();
+      block_select<SideTeam, false>(hist, NB, (uint32_t)krem, m);
       if (!m->sel_found) {
-        if (threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusSelect);
+        if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
         return;
       }
       prefix = (prefix << D) | m->sel_bin;
       plen += D;
       krem -= (int)m->sel_cum;
       count = (int)m->sel_cnt;
-      __syncthreads();
+      SideTeam::sync();
     }
     const bool final_mode = count == krem;
-    if (threadIdx.x == 0) m->counter = 0;
-    __syncthreads();
+    if (SideTeam::tid() == 0) m->counter = 0;
+    SideTeam::sync();
     cta_filter(rc, rs, prefix, plen, final_mode, ent);
-    __syncthreads();
+    SideTeam::sync();
     if (!final_mode) {
       const int ne = min((int)m->counter, kCapSB);
-      __syncthreads();
-      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+      SideTeam::sync();
+      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                               &p.hdr->status);
-      smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
     }
-    post_process<VT, SCALE>(p, rc, smem, m);
+    post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
   }
 
   // ---- copy chunk ia of a k >= n row (every element is selected)
-  __device__ void all_item(int r, const RowCtx& rc, int ia) {
+  __device__ void all_item(int r, const RowCtx& rc, const ItemDesc& d) {
     RowState* rs = p.rs + r;
-    const int warp = threadIdx.x >> 5;
-    WarpBuf ob{out_sink(warp), 0};
+    const int warp = ConsTeam::wid();
+    WarpBuf ob{out_sink<ConsTeam>(), 0};
     uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
     auto fl = [&](const WarpBuf& s) { flush_out<VT>(p, s, ctr, rc.out_off, rc.k); };
-    const int64_t a = (int64_t)ia * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
-    stream_chunk(
-        rc, a, b, [] {},
+    consume_chunk(
+        rc, d, [] {},
         [&](uint32_t bits, int64_t pos, bool ok) { sink_push(ob, kSinkOut, ok, make_entry(bits, pos), fl); },
         [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
@@ -1218,12 +1236,12 @@ struct Engine {
   // thread after the item's closing barrier, without waiting for the result
   // (the release's latency overlaps the next item).
   __device__ void defer_release(int r) {
-    if (threadIdx.x == 0) m->rel_row = r;
+    if (ConsTeam::tid() == 0) m->rel_row = r;
   }
 
   // ---- FIN item: wait for the row's chunk items, then finish the row
   __device__ void fin_item(int r, const RowCtx& rc) {
-    if (threadIdx.x == 0) {
+    if (SideTeam::tid() == 0) {
       const int32_t* t = &p.rs[r].fticket;
       uint32_t it = 0;
       while (ld_acquire(t) < rc.fin_wait) {
@@ -1234,14 +1252,14 @@ struct Engine {
         __nanosleep(128);
       }
     }
-    __syncthreads();
+    SideTeam::sync();
     finish_row(r);
   }
 
   // ---- sample item of a pre-filter row: publish the threshold
   __device__ void sample_item(int r, const RowCtx& rc) {
     const uint32_t T = sample_threshold(rc);
-    if (threadIdx.x == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
+    if (SideTeam::tid() == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
   }
 
   // ---- filter item of a pre-filter row: keys <= T into the candidates.
@@ -1250,11 +1268,11 @@ struct Engine {
   // the keys <= T.  Only vectors with a passing element take the exact
   // integer-key test and the warp-scan compaction into the warp's buffer.
   template <bool LARGEST>
-  __device__ void pf_item_t(int r, const RowCtx& rc, int ib) {
+  __device__ void pf_item_t(int r, const RowCtx& rc, const ItemDesc& d) {
     RowState* rs = p.rs + r;
     uint32_t T = 0;
     auto pre = [&]() {
-      if (threadIdx.x == 0 && m->t_row != r) {
+      if (ConsTeam::tid() == 0 && m->t_row != r) {
         uint64_t v = ld_acquire_u64(&rs->tready);
         for (uint32_t it = 0; !(v >> 32); ++it) {
           if (it > p.spin_limit) {
@@ -1267,18 +1285,17 @@ struct Engine {
         m->t_val = (uint32_t)v;
         m->t_row = r;
       }
-      __syncthreads();
+      ConsTeam::sync();
       T = m->t_val;
     };
-    const int warp = threadIdx.x >> 5;
+    const int warp = ConsTeam::wid();
     const unsigned lane = threadIdx.x & 31u;
     constexpr int kCap = kSinkPf;
-    WarpBuf cb{reinterpret_cast<uint64_t*>(smem + kSinkPfOff) + warp * kCap, 0};
+    WarpBuf cb{reinterpret_cast<uint64_t*>(smem) + warp * kCap, 0};
     uint32_t* ctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
     uint64_t* dst = p.cand + rc.cand_off;
     const uint32_t flip = rc.flip;
     const float sc = rc.scaler;
-    const int64_t a = (int64_t)ib * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
     // lane's hit mask over up to VEC elements -> warp buffer
     auto push = [&](uint32_t hm, uint32_t e0bits_unused, auto elem_bits, int64_t pos0) {
       (void)e0bits_unused;
@@ -1303,8 +1320,8 @@ struct Engine {
       }
       cb.n += tot;
     };
-    stream_chunk(
-        rc, a, b, pre,
+    consume_chunk(
+        rc, d, pre,
         [&](uint32_t bits, int64_t pos, bool ok) {
           const bool hit = ok && sel_key<VT, SCALE>(bits, flip, sc) <= T;
           if (__any_sync(kFull, hit)) push(hit ? 1u : 0u, 0u, [&](int) { return bits; }, pos);
@@ -1363,38 +1380,37 @@ struct Engine {
     defer_release(r);
   }
 
-  __device__ void pf_item(int r, const RowCtx& rc, int ib) {
-    if (p.flags & kFlagLargest) pf_item_t<true>(r, rc, ib);
-    else pf_item_t<false>(r, rc, ib);
+  __device__ void pf_item(int r, const RowCtx& rc, const ItemDesc& d) {
+    if (p.flags & kFlagLargest) pf_item_t<true>(r, rc, d);
+    else pf_item_t<false>(r, rc, d);
   }
 
   // ---- histogram item of a radix row: first digit of chunk ia
-  __device__ void h_item(int r, const RowCtx& rc, int ia) {
+  __device__ void h_item(int r, const RowCtx& rc, const ItemDesc& d) {
     const int D1 = p.D1;
     const int NB = 1 << D1;
     const int s = rc.slot_use % p.S;
     const uint32_t use = (uint32_t)(rc.slot_use / p.S);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kHistOff);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kHistOff);  // consumer area
     uint32_t* ghist = p.hist_ring + (size_t)s * ((size_t)1 << kMaxD1);
-    if (threadIdx.x == 0) m->bcast = use == 0 ? 1 : (int)spin_until_ge(p.slot_gen + s, use);
-    for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) *reinterpret_cast<uint4*>(hist + i) = make_uint4(0, 0, 0, 0);
-    __syncthreads();
+    if (ConsTeam::tid() == 0) m->bcast = use == 0 ? 1 : (int)spin_until_ge(p.slot_gen + s, use);
+    for (int i = ConsTeam::tid() * 4; i < NB; i += ConsTeam::kSize * 4) *reinterpret_cast<uint4*>(hist + i) = make_uint4(0, 0, 0, 0);
+    ConsTeam::sync();
     const bool slot_ok = m->bcast != 0;
     const int shift = K::KB - D1;
-    const int64_t a = (int64_t)ia * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
     const uint32_t flip = rc.flip;
     const float sc = rc.scaler;
     bool agg = false;
-    stream_chunk(
-        rc, a, b, [] {},
+    consume_chunk(
+        rc, d, [] {},
         [&](uint32_t bits, int64_t, bool ok) { hist_add_agg(hist, sel_key<VT, SCALE>(bits, flip, sc) >> shift, ok); },
         [&](const uint4& x, int64_t, bool ok) {
 #pragma unroll
           for (int e = 0; e < VEC; ++e) hist_add(hist, sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) >> shift, ok, e, agg);
         });
-    __syncthreads();
+    ConsTeam::sync();
     if (slot_ok) {
-      for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) {
+      for (int i = ConsTeam::tid() * 4; i < NB; i += ConsTeam::kSize * 4) {
         const uint4 v = *reinterpret_cast<const uint4*>(hist + i);
         if (v.x) atomicAdd(ghist + i + 0, v.x);
         if (v.y) atomicAdd(ghist + i + 1, v.y);
@@ -1403,20 +1419,20 @@ struct Engine {
       }
     }
     __threadfence();
-    __syncthreads();
+    ConsTeam::sync();
     RowState* rs = p.rs + r;
-    if (threadIdx.x == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
-    __syncthreads();
+    if (ConsTeam::tid() == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
+    ConsTeam::sync();
     if (!m->bcast2) return;
     // Last histogram item of the row: select the first digit's bin.
     __threadfence();
-    block_select<true>(ghist, NB, (uint32_t)rc.k, m);
+    block_select<ConsTeam, true>(ghist, NB, (uint32_t)rc.k, m);
     const bool found = m->sel_found != 0;
     const uint32_t bin = m->sel_bin, cum = m->sel_cum, cnt = m->sel_cnt;
-    for (int i = threadIdx.x * 4; i < NB; i += kThreads * 4) *reinterpret_cast<uint4*>(ghist + i) = make_uint4(0, 0, 0, 0);
+    for (int i = ConsTeam::tid() * 4; i < NB; i += ConsTeam::kSize * 4) *reinterpret_cast<uint4*>(ghist + i) = make_uint4(0, 0, 0, 0);
     __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    ConsTeam::sync();
+    if (ConsTeam::tid() == 0) {
       int mode;
       const int krem = rc.k - (int)cum;
       if (!found || !slot_ok) {
@@ -1443,23 +1459,23 @@ struct Engine {
   }
 
   // ---- filter item of a radix row
-  __device__ void f_item(int r, const RowCtx& rc, int ib) {
+  __device__ void f_item(int r, const RowCtx& rc, const ItemDesc& d) {
     RowState* rs = p.rs + r;
-    if (threadIdx.x == 0) {
+    if (ConsTeam::tid() == 0) {
       int mode = kModeNone;
       if (spin_until_ge(reinterpret_cast<const uint32_t*>(&rs->ready), 1u)) mode = __ldcg(&rs->mode);
       m->st_mode = mode;
       m->st_prefix = ld_cg_u64(&rs->prefix);
     }
-    __syncthreads();
+    ConsTeam::sync();
     const int mode = m->st_mode;
     if (mode == kModeFinal || mode == kModeSB || mode == kModeCand) {
       const uint32_t prefix = (uint32_t)m->st_prefix;
       const int shift = K::KB - p.D1;
       const bool final_mode = mode == kModeFinal;
-      const int warp = threadIdx.x >> 5;
-      WarpBuf cb{cand_sink(warp), 0};
-      WarpBuf ob{out_sink(warp), 0};
+      const int warp = ConsTeam::wid();
+      WarpBuf cb{cand_sink<ConsTeam>(), 0};
+      WarpBuf ob{out_sink<ConsTeam>(), 0};
       uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
       uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
       uint64_t* dst = p.cand + rc.cand_off;
@@ -1474,8 +1490,7 @@ struct Engine {
         sink_push(ob, kSinkOut, to_out, make_entry(bits, pos), flo);
         sink_push(cb, kSinkCand, to_cand, make_entry(bits, pos), flc);
       };
-      const int64_t a = (int64_t)ib * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
-      stream_chunk(rc, a, b, [] {}, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      consume_chunk(rc, d, [] {}, one, [&](const uint4& x, int64_t pos0, bool ok) {
         bool any = false;
 #pragma unroll
         for (int e = 0; e < VEC; ++e) any |= ok && (sel_key<VT, SCALE>(vec_elem<ES>(x, e), flip, sc) >> shift) <= prefix;
@@ -1486,14 +1501,17 @@ struct Engine {
       });
       if (ob.n) flo(ob);
       if (cb.n) flc(cb);
+    } else {
+      // nothing to filter (the row continues in phase B, or timed out): the
+      // producer has issued this chunk's copies all the same, so drain them
+      consume_chunk(rc, d, [] {}, [](uint32_t, int64_t, bool) {}, [](const uint4&, int64_t, bool) {});
     }
-    do_release();  // the previous item's counter, if no stream ran above
     defer_release(r);
   }
 
   // Hands a row to phase B.
   __device__ void to_phase_b(int r, int src, int src_len, uint64_t prefix, int plen, int krem, int count) {
-    if (threadIdx.x == 0) {
+    if (SideTeam::tid() == 0) {
       RowState* rs = p.rs + r;
       rs->src = src;
       rs->src_len = src_len;
@@ -1514,7 +1532,7 @@ struct Engine {
     const RowCtx rc = load_row<VT, SCALE>(p, r);
     RowState* rs = p.rs + r;
     __threadfence();
-    if (threadIdx.x == 0) {
+    if (SideTeam::tid() == 0) {
       m->st_mode = rc.kind == kKindAll ? kModeAll : __ldcg(&rs->mode);
       m->st_krem = __ldcg(&rs->krem);
       m->st_count = __ldcg(&rs->count);
@@ -1522,7 +1540,7 @@ struct Engine {
       m->st_prefix = ld_cg_u64(&rs->prefix);
       m->st_candn = __ldcg(&rs->cand_count);
     }
-    __syncthreads();
+    SideTeam::sync();
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
     auto get = [&](int i, uint32_t& bits, int64_t& pos) {
       const uint64_t e = ent[i];
@@ -1533,14 +1551,14 @@ struct Engine {
     if (rc.kind == kKindGridPref) {
       const int c = m->st_candn;
       if (c >= rc.k && c <= kCapSB) {
-        for (int i = threadIdx.x; i < c; i += kThreads) ent[i] = ld_cg_u64(cand + i);
-        __syncthreads();
+        for (int i = SideTeam::tid(); i < c; i += SideTeam::kSize) ent[i] = ld_cg_u64(cand + i);
+        SideTeam::sync();
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+        smem_resolve<SideTeam, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                                 &p.hdr->status);
-        smem_emit<VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
-        post_process<VT, SCALE>(p, rc, smem, m);
+        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
       } else if (c >= rc.k && c <= rc.cand_cap) {
         to_phase_b(r, 1, c, 0, 0, rc.k, c);
       } else {
@@ -1551,20 +1569,20 @@ struct Engine {
     const int mode = m->st_mode;
     if (mode == kModeSB) {
       const int ne = min(m->st_candn, kCapSB);
-      for (int i = threadIdx.x; i < ne; i += kThreads) ent[i] = ld_cg_u64(cand + i);
+      for (int i = SideTeam::tid(); i < ne; i += SideTeam::kSize) ent[i] = ld_cg_u64(cand + i);
       uint64_t prefix = m->st_prefix;
       int plen = m->st_plen, krem = m->st_krem;
-      __syncthreads();
-      smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+      SideTeam::sync();
+      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                               &p.hdr->status);
-      smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
-      post_process<VT, SCALE>(p, rc, smem, m);
+      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
     } else if (mode == kModeCand) {
       to_phase_b(r, 1, min(m->st_candn, rc.cand_cap), m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeDefer) {
       to_phase_b(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeFinal || mode == kModeAll) {
-      post_process<VT, SCALE>(p, rc, smem, m);
+      post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
     }
   }
 
@@ -1581,15 +1599,15 @@ struct Engine {
     if (src == 1) {
       const uint64_t* cand = p.cand + rc.cand_off;
       const int64_t cnt = b - a;
-      const int64_t iters = (cnt + kThreads - 1) / kThreads;
+      const int64_t iters = (cnt + FullTeam::kSize - 1) / FullTeam::kSize;
       for (int64_t it = 0; it < iters; ++it) {
-        const int64_t i = a + it * kThreads + threadIdx.x;
+        const int64_t i = a + it * FullTeam::kSize + FullTeam::tid();
         const bool ok = i < b;
         const uint64_t e = ok ? ld_cg_u64(cand + i) : 0ull;
         fn((uint32_t)(e >> 32), (int64_t)(uint32_t)e, ok);
       }
     } else {
-      for_range_v<ES, U>(p.val_in, rc.in_off, a, b, fn, [&](const uint4& x, int64_t pos0, bool ok) {
+      for_range_v<FullTeam, ES, U>(p.val_in, rc.in_off, a, b, fn, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) fn(vec_elem<ES>(x, e), pos0 + e, ok);
       });
@@ -1600,7 +1618,7 @@ struct Engine {
   // (0: rows that still need a histogram level, 1: rows due for the final
   // filter).  Returns the number of chunks.
   __device__ int pb_table(PBTable* t, int nG, int want) {
-    if (threadIdx.x == 0) {
+    if (FullTeam::tid() == 0) {
       int c = 0;
       for (int i = 0; i < nG; ++i) {
         const int r = p.large_list[i];
@@ -1614,14 +1632,14 @@ struct Engine {
       }
       t->c0[nG] = c;
     }
-    __syncthreads();
+    FullTeam::sync();
     return t->c0[nG];
   }
 
   __device__ void phase_b() {
     PBTable* t = reinterpret_cast<PBTable*>(m->pbtab);
     for (int round = 0; round < 64; ++round) {
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       const int nL = __ldcg(&p.hdr->nlarge);
       if (nL <= 0) return;
       const int nG = min(nL, kPhaseBSlots);
@@ -1629,14 +1647,14 @@ struct Engine {
       // slot is cleared here (the call clears the ring only for radix rows)
       for (int i = blockIdx.x; i < nG; i += gridDim.x) {
         uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
-        for (int j = threadIdx.x; j < 4096; j += kThreads) gh[j] = 0;
-        if (threadIdx.x == 0) {
+        for (int j = FullTeam::tid(); j < 4096; j += FullTeam::kSize) gh[j] = 0;
+        if (FullTeam::tid() == 0) {
           RowState* rs = p.rs + p.large_list[i];
           const int cnt = __ldcg(&rs->count), kr = __ldcg(&rs->krem);
           rs->final_pass = (cnt == kr || cnt <= kCapSB) ? 1 : 0;
         }
       }
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- histogram of the next 12-bit digit
       int total = pb_table(t, nG, 0);
       uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
@@ -1653,8 +1671,8 @@ struct Engine {
         const int W = K::KB + rc.IB;
         const int D = min(12, W - plen);
         const int NB = 1 << D;
-        for (int j = threadIdx.x; j < NB; j += kThreads) hist[j] = 0;
-        __syncthreads();
+        for (int j = FullTeam::tid(); j < NB; j += FullTeam::kSize) hist[j] = 0;
+        FullTeam::sync();
         const int sh = W - plen, sd = W - plen - D;
         const uint32_t dm = (uint32_t)NB - 1u;
         const int64_t a = (int64_t)(w - t->c0[i]) * kPhaseBChunk, b = min((int64_t)len, a + kPhaseBChunk);
@@ -1662,13 +1680,13 @@ struct Engine {
           const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
           hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
         });
-        __syncthreads();
+        FullTeam::sync();
         uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
-        for (int j = threadIdx.x; j < NB; j += kThreads)
+        for (int j = FullTeam::tid(); j < NB; j += FullTeam::kSize)
           if (hist[j]) atomicAdd(gh + j, hist[j]);
-        __syncthreads();
+        FullTeam::sync();
       }
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- bin selection, one CTA per row
       for (int i = blockIdx.x; i < nG; i += gridDim.x) {
         const int r = p.large_list[i];
@@ -1681,12 +1699,12 @@ struct Engine {
         const int NB = 1 << D;
         uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
         const int krem = __ldcg(&rs->krem);
-        block_select<true>(gh, NB, (uint32_t)krem, m);
+        block_select<FullTeam, true>(gh, NB, (uint32_t)krem, m);
         const bool found = m->sel_found != 0;
         const uint32_t bin = m->sel_bin, cum = m->sel_cum, cnt = m->sel_cnt;
-        for (int j = threadIdx.x; j < NB; j += kThreads) gh[j] = 0;
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        for (int j = FullTeam::tid(); j < NB; j += FullTeam::kSize) gh[j] = 0;
+        FullTeam::sync();
+        if (FullTeam::tid() == 0) {
           if (!found) {
             atomicOr(&p.hdr->status, kStatusSelect);
             rs->count = krem;  // give up on this row: finish what is there
@@ -1699,12 +1717,12 @@ struct Engine {
             rs->final_pass = ((int)cnt == krem - (int)cum || (int)cnt <= kCapSB) ? 1 : 0;
           }
         }
-        __syncthreads();
+        FullTeam::sync();
       }
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- final filter for the rows that are due
       total = pb_table(t, nG, 1);
-      const int warp = threadIdx.x >> 5;
+      const int warp = FullTeam::wid();
       for (int w = blockIdx.x; w < total; w += gridDim.x) {
         int i = 0;
         while (t->c0[i + 1] <= w) ++i;
@@ -1718,8 +1736,8 @@ struct Engine {
         const bool final_mode = __ldcg(&rs->count) == __ldcg(&rs->krem);
         const int W = K::KB + rc.IB;
         const int sh = W - plen;
-        WarpBuf cb{cand_sink(warp), 0};
-        WarpBuf ob{out_sink(warp), 0};
+        WarpBuf cb{cand_sink<FullTeam>(), 0};
+        WarpBuf ob{out_sink<FullTeam>(), 0};
         uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->sb_count);
         uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
         uint64_t* dst = p.pb_sb + (size_t)i * kCapSB;
@@ -1734,9 +1752,9 @@ struct Engine {
         });
         if (ob.n) flo(ob);
         if (cb.n) flc(cb);
-        __syncthreads();
+        FullTeam::sync();
       }
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- finish the rows that were filtered
       uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
       for (int i = blockIdx.x; i < nG; i += gridDim.x) {
@@ -1748,25 +1766,25 @@ struct Engine {
         if (count != krem0) {
           const int ne = min(__ldcg(&rs->sb_count), kCapSB);
           const uint64_t* sb = p.pb_sb + (size_t)i * kCapSB;
-          for (int j = threadIdx.x; j < ne; j += kThreads) ent[j] = ld_cg_u64(sb + j);
+          for (int j = FullTeam::tid(); j < ne; j += FullTeam::kSize) ent[j] = ld_cg_u64(sb + j);
           uint64_t prefix = ld_cg_u64(&rs->prefix);
           int plen = __ldcg(&rs->plen), krem = krem0;
-          __syncthreads();
+          FullTeam::sync();
           auto get = [&](int j, uint32_t& bits, int64_t& pos) {
             const uint64_t e = ent[j];
             bits = (uint32_t)(e >> 32);
             pos = (int64_t)(uint32_t)e;
           };
-          smem_resolve<VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+          smem_resolve<FullTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                               &p.hdr->status);
-          smem_emit<VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+          smem_emit<FullTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
         }
-        post_process<VT, SCALE>(p, rc, smem, m);
-        if (threadIdx.x == 0) rs->final_pass = 2;  // done
+        post_process<FullTeam, VT, SCALE>(p, rc, smem, m);
+        if (FullTeam::tid() == 0) rs->final_pass = 2;  // done
       }
-      grid_barrier(p.hdr, p.spin_limit);
+      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- drop the finished rows from the list (CTA 0)
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (blockIdx.x == 0 && FullTeam::tid() == 0) {
         int w = 0;
         for (int i = 0; i < nL; ++i) {
           const int r = p.large_list[i];
@@ -1777,7 +1795,7 @@ struct Engine {
         __threadfence();
       }
     }
-    if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(&p.hdr->status, kStatusLevels);
+    if (FullTeam::tid() == 0 && blockIdx.x == 0) atomicOr(&p.hdr->status, kStatusLevels);
   }
 };
 
@@ -1809,30 +1827,167 @@ __device__ __forceinline__ bool decode_item(int q, int NA, int NB, int L, int& i
   return false;
 }
 
+// Item geometry of a claim: which row, A or B item, chunk, FIN.
+struct ItemRef {
+  int32_t row, sub, isA, fin;
+};
+
+__device__ __forceinline__ ItemRef resolve_item(const EngineParams& p, int q, int NA, int NB, int lag, int una, int unc,
+                                                int ufin) {
+  ItemRef it{0, 0, 0, 0};
+  int idx;
+  it.isA = decode_item(q, NA, NB, lag, idx);
+  if (it.isA) {
+    it.row = p.uniform ? idx / una : p.a_row[idx];
+    it.sub = idx;  // made row-relative once the row's a0 is known
+  } else if (p.uniform) {
+    uniform_b_item(idx, p.B, unc, ufin, p.fin_delay, &it.row, &it.sub, &it.fin);
+  } else {
+    const int32_t v = p.b_row[idx];
+    it.row = v & 0x7FFFFFFF;
+    it.fin = (v >> 31) & 1;
+    it.sub = idx;  // made row-relative once the row's b0 is known
+  }
+  return it;
+}
+
+__device__ __forceinline__ bool is_streaming(int kind, int isA, int fin) {
+  return isA ? (kind == kKindAll || kind == kKindGridRadix)
+             : (!fin && (kind == kKindGridPref || kind == kKindGridRadix));
+}
+
+// Producer (one thread): claims items in order, routes streaming items to
+// the consumer queue and the rest to the side queue, and issues the bulk
+// copies of each streaming chunk into the ring as slots drain.
+template <int VT, bool SCALE>
+__device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, int lag, int una, int unc, int ufin) {
+  constexpr int ES = KT<VT, SCALE>::ES, VEC = KT<VT, SCALE>::VEC;
+  const int NQ = NA + NB;
+  uint32_t g = 0, ci = 0, si = 0;
+  auto push = [&](uint64_t* full, uint64_t* empty, ItemDesc* slots, uint32_t& i, const ItemDesc& d) {
+    const uint32_t slot = i % kQ;
+    if (i >= (uint32_t)kQ) {
+      const uint32_t parity = ((i / kQ) - 1u) & 1u;
+      uint32_t it = 0;
+      while (!mbar_try_wait(&empty[slot], parity)) {
+        if (++it > p.spin_limit) {
+          atomicOr(&p.hdr->status, kStatusTimeout);
+          break;
+        }
+      }
+    }
+    slots[slot] = d;
+    mbar_arrive(&full[slot]);
+    ++i;
+  };
+  while (true) {
+    const int q = (int)atomicAdd(&p.hdr->qhead, 1u);
+    ItemDesc d{};
+    if (q >= NQ) {
+      d.q = -1;
+      push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
+      push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
+      break;
+    }
+    const ItemRef ir = resolve_item(p, q, NA, NB, lag, una, unc, ufin);
+    const RowCtx rc = load_row<VT, SCALE>(p, ir.row);
+    d.q = q;
+    d.row = ir.row;
+    d.isA = ir.isA;
+    d.fin = ir.fin;
+    d.sub = ir.isA ? ir.sub - rc.a0 : (p.uniform ? ir.sub : ir.sub - rc.b0);
+    if (!is_streaming(rc.kind, ir.isA, ir.fin)) {
+      push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
+      continue;
+    }
+    // chunk geometry: the aligned middle goes through the ring
+    const int64_t a = (int64_t)d.sub * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
+    const char* row = static_cast<const char*>(p.val_in) + rc.in_off * ES;
+    int64_t head = 0, nvec = 0;
+    if (b > a) {
+      const uintptr_t addr_a = reinterpret_cast<uintptr_t>(row + a * ES);
+      head = (int64_t)(((16u - (unsigned)(addr_a & 15u)) & 15u) / ES);
+      if (head > b - a) head = b - a;
+      nvec = (b - a - head) / VEC;
+    }
+    d.a = a;
+    d.b = b;
+    d.va = a + head;
+    d.nvec = nvec;
+    d.nst = (int32_t)((nvec + kStageVecs - 1) / kStageVecs);
+    d.g0 = g;
+    push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
+    const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
+    uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
+    for (int i = 0; i < d.nst; ++i, ++g) {
+      const uint32_t slot = g % kStages;
+      if (g >= (uint32_t)kStages) {
+        const uint32_t parity = ((g / kStages) - 1u) & 1u;
+        uint32_t it = 0;
+        while (!mbar_try_wait(&ctl->empty[slot], parity)) {
+          if (++it > p.spin_limit) {
+            atomicOr(&p.hdr->status, kStatusTimeout);
+            break;
+          }
+        }
+      }
+      const int64_t v0 = (int64_t)i * kStageVecs;
+      const uint32_t bytes = (uint32_t)min((int64_t)kStageVecs, nvec - v0) * 16u;
+      mbar_expect_tx(&ctl->full[slot], bytes);
+      bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &ctl->full[slot]);
+    }
+  }
+}
+
+// Pops the team's next item (every thread of the team calls it).
+template <class Tm>
+__device__ __forceinline__ ItemDesc pop_item(uint64_t* full, uint64_t* empty, const ItemDesc* slots, uint32_t i,
+                                             const EngineParams& p) {
+  const uint32_t slot = i % kQ;
+  const uint32_t parity = (i / kQ) & 1u;
+  uint32_t it = 0;
+  while (!mbar_try_wait(&full[slot], parity)) {
+    if (++it > p.spin_limit) {
+      if (Tm::tid() == 0) atomicOr(&p.hdr->status, kStatusTimeout);
+      break;
+    }
+  }
+  const ItemDesc d = slots[slot];
+  Tm::sync();
+  if (Tm::tid() == 0) mbar_arrive(&empty[slot]);
+  return d;
+}
+
 template <int VT, bool SCALE>
 __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __grid_constant__ EngineParams p) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  Engine<VT, SCALE> e(p, smem);
-  Misc* m = e.m;
+  extern __shared__ __align__(128) uint8_t smem[];
+  Ctrl* ctl = ctrl_of(smem);
   if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kStages; ++i) {
-      mbar_init(&m->mbar[i], 1);
-      mbar_init(&m->mbar_empty[i], kWarps);
+      mbar_init(&ctl->full[i], 1);
+      mbar_init(&ctl->empty[i], ConsTeam::kWarps);
+    }
+    for (int i = 0; i < kQ; ++i) {
+      mbar_init(&ctl->cq_full[i], 1);
+      mbar_init(&ctl->cq_empty[i], 1);
+      mbar_init(&ctl->sq_full[i], 1);
+      mbar_init(&ctl->sq_empty[i], 1);
     }
     mbar_fence_init();
-    m->rel_row = -1;
-    m->t_row = -1;
-    m->ring_dirty = 0;
+    for (Misc* mm : {cons_misc(smem), side_misc(smem)}) {
+      mm->rel_row = -1;
+      mm->t_row = -1;
+    }
   }
   __syncthreads();
   int NA, NB, lag;
-  int ukind = 0, una = 1, unc = 0, ufin = 0;
+  int una = 1, unc = 0, ufin = 0;
   if (p.uniform) {
-    ukind = row_kind(p.u_n, p.u_k);
-    una = row_na(ukind, p.u_n, p.CH, p.CHR);
-    unc = row_nbc(ukind, p.u_n, p.CH, p.CHR);
-    ufin = row_fin(ukind);
+    const int kind = row_kind(p.u_n, p.u_k);
+    una = row_na(kind, p.u_n, p.CH, p.CHR);
+    unc = row_nbc(kind, p.u_n, p.CH, p.CHR);
+    ufin = row_fin(kind);
     NA = p.B * una;
     NB = p.B * (unc + ufin);
     lag = p.lag;
@@ -1841,67 +1996,55 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     NB = __ldcg(&p.hdr->nb);
     lag = __ldcg(&p.hdr->lag);
   }
-  const int NQ = NA + NB;
-  if (threadIdx.x == 0) m->next_q = (int)atomicAdd(&p.hdr->qhead, 1u);
-  __syncthreads();
-  int q = m->next_q;
-  while (q < NQ) {
-    // the previous chunk item's counter is released during this item
-    e.pending_rel = m->rel_row;
-    __syncthreads();
-    if (threadIdx.x == 0) m->rel_row = -1;
-    uint32_t nq = 0;
-    if (threadIdx.x == 0) nq = atomicAdd(&p.hdr->qhead, 1u);
-    int idx;
-    const bool isA = decode_item(q, NA, NB, lag, idx);
-    int r, sub = 0, fin = 0;
-    if (isA) {
-      r = p.uniform ? idx / una : p.a_row[idx];
-    } else if (p.uniform) {
-      uniform_b_item(idx, p.B, unc, ufin, p.fin_delay, &r, &sub, &fin);
-    } else {
-      const int32_t v = p.b_row[idx];
-      r = v & 0x7FFFFFFF;
-      fin = (v >> 31) & 1;
-    }
-    const RowCtx rc = load_row<VT, SCALE>(p, r);
-    if (!p.uniform && !isA && !fin) sub = idx - rc.b0;
-    const bool streaming = isA ? (rc.kind == kKindAll || rc.kind == kKindGridRadix)
-                               : (!fin && (rc.kind == kKindGridPref || rc.kind == kKindGridRadix));
-    if (!streaming) e.do_release();
-    if (isA) {
-      switch (rc.kind) {
-        case kKindSmem:
-          if (threadIdx.x == 0) m->ring_dirty = 1;
-          e.smem_row(r, rc);
-          break;
-        case kKindCta:
-          if (threadIdx.x == 0) m->ring_dirty = 1;
-          e.cta_row(r, rc);
-          break;
-        case kKindAll: e.all_item(r, rc, idx - rc.a0); break;
-        case kKindGridPref:
-          if (threadIdx.x == 0) m->ring_dirty = 1;
-          e.sample_item(r, rc);
-          break;
-        case kKindGridRadix: e.h_item(r, rc, idx - rc.a0); break;
-        default: break;
+  const int warp = threadIdx.x >> 5;
+  if (warp == kProducerWarp) {
+    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin);
+  } else if (warp < kConsWarps) {
+    // consumer team: streaming items
+    Engine<VT, SCALE> e(p, smem, smem + kConsAreaOff, cons_misc(smem));
+    Misc* m = e.m;
+    for (uint32_t i = 0;; ++i) {
+      const ItemDesc d = pop_item<ConsTeam>(ctl->cq_full, ctl->cq_empty, ctl->cq, i, p);
+      // the previous item's chunk counter is released during this one
+      e.pending_rel = m->rel_row;
+      ConsTeam::sync();
+      if (ConsTeam::tid() == 0) m->rel_row = -1;
+      if (d.q < 0) break;
+      const RowCtx rc = load_row<VT, SCALE>(p, d.row);
+      if (d.isA) {
+        if (rc.kind == kKindAll) e.all_item(d.row, rc, d);
+        else e.h_item(d.row, rc, d);
+      } else if (rc.kind == kKindGridPref) {
+        e.pf_item(d.row, rc, d);
+      } else {
+        e.f_item(d.row, rc, d);
       }
-    } else if (fin) {
-      if (threadIdx.x == 0) m->ring_dirty = 1;
-      e.fin_item(r, rc);
-    } else if (rc.kind == kKindGridPref) {
-      e.pf_item(r, rc, sub);
-    } else if (rc.kind == kKindGridRadix) {
-      e.f_item(r, rc, sub);
+      ConsTeam::sync();
     }
-    __syncthreads();
-    if (threadIdx.x == 0) m->next_q = (int)nq;
-    __syncthreads();
-    q = m->next_q;
+    e.do_release();
+  } else {
+    // side team: samples, single-item rows, FIN items
+    Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
+    for (uint32_t i = 0;; ++i) {
+      const ItemDesc d = pop_item<SideTeam>(ctl->sq_full, ctl->sq_empty, ctl->sq, i, p);
+      if (d.q < 0) break;
+      const RowCtx rc = load_row<VT, SCALE>(p, d.row);
+      if (d.isA) {
+        switch (rc.kind) {
+          case kKindSmem: e.smem_row(d.row, rc); break;
+          case kKindCta: e.cta_row(d.row, rc); break;
+          case kKindGridPref: e.sample_item(d.row, rc); break;
+          default: break;
+        }
+      } else if (d.fin) {
+        e.fin_item(d.row, rc);
+      }
+      SideTeam::sync();
+    }
   }
-  e.pending_rel = m->rel_row;
-  e.do_release();
+  __syncthreads();
+  // phase B: the whole CTA, scratch in the side area
+  Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
   e.phase_b();
 }
 

@@ -36,14 +36,14 @@ enum : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 constexpr int kThreads = 1024;           // one CTA per SM: 24 consumer, 7 side, 1 producer warp
 constexpr int kCtasPerSM = 1;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCapSB = 10240;            // candidates a finisher resolves in smem (80 KB)
+constexpr int kCapSB = 7168;             // candidates a finisher resolves in smem (56 KB)
 constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
 constexpr int kCtaRowCap = 1 << 18;      // rows this short are selected by one CTA
 constexpr int kCapSort = 8192;           // outputs a finisher sorts in smem (64 KB)
 constexpr int kMaxD1 = 12;               // widest first digit (16 KB smem hist)
 constexpr int kMinD1 = 8;
 constexpr int kPrefRatio = 64;           // pre-filter rows with k * 64 <= n
-constexpr int kSampleMax = 16384;        // sampled keys per row (64 KB smem)
+constexpr int kSampleMax = 8192;         // sampled keys per row (32 KB smem)
 constexpr int kSampleMin = 1024;
 constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
 constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)
@@ -130,7 +130,8 @@ struct alignas(16) Header {
   uint32_t pbhead;      // phase-B claim counter
   int64_t cand_total;   // candidate entries planned
   int64_t sort_total;   // sort-scratch entries planned
-  int32_t pad[50];
+  int32_t fin_tail;     // FIN items at the end of the claim order
+  int32_t pad[49];
 };
 static_assert(sizeof(Header) == 256, "Header layout");
 

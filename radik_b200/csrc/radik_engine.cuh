@@ -196,14 +196,14 @@ __device__ __forceinline__ uint32_t out_key_inv(uint32_t k, bool ascend) {
 //   consumer area  per-warp staging buffers / first-digit histogram
 //   side area      sampled keys, candidate entries, sort and resolve scratch
 //   control        per-team scratch (Misc), ring and queue mbarriers
-constexpr int kStages = 4;
+constexpr int kStages = 5;
 constexpr int kStageVecs = 24 * 32 * 2;                 // two 16-byte vectors per consumer thread
 constexpr int kStageBytes = kStageVecs * 16;            // 24 KB
-constexpr int kRingBytes = kStages * kStageBytes;       // 96 KB
+constexpr int kRingBytes = kStages * kStageBytes;       // 120 KB
 constexpr int kConsAreaOff = kRingBytes;
 constexpr int kConsAreaBytes = 24 * 1024;
 constexpr int kSideAreaOff = kConsAreaOff + kConsAreaBytes;
-constexpr int kSideAreaBytes = 96 * 1024;
+constexpr int kSideAreaBytes = 72 * 1024;
 constexpr int kCtrlOff = kSideAreaOff + kSideAreaBytes;  // 216 KB
 constexpr int kSinkCand = 96;                           // filter items: candidate entries per warp
 constexpr int kSinkOut = 32;                            // filter / copy items: output entries per warp
@@ -219,6 +219,7 @@ static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B stagin
 static_assert((4 << kMaxD1) <= kConsAreaBytes, "histogram");
 static_assert(kResolveHistOff + 16384 <= kSideAreaBytes, "finisher area");
 static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
+static_assert(32 * 128 * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert(kSampleHistOff + 16384 <= kSideAreaBytes, "sample area");
 
 struct Misc {
@@ -252,17 +253,21 @@ struct alignas(16) ItemDesc {
   int32_t sub;   // chunk index within the row
   int32_t nst;   // bulk-copy stages of a streaming item
   uint32_t g0;   // its first global ring stage
-  int32_t pad;
+  uint32_t thr;  // pre-filter threshold, if the producer found it published
+  int32_t thr_ok;
+  int32_t pad[3];
   int64_t a, b;  // positions [a, b) of the chunk
   int64_t va;    // first 16-byte aligned position
   int64_t nvec;  // aligned 16-byte vectors from va
 };
 constexpr int kQ = 4;  // queue slots per team
+constexpr int kSideCandMax = 1 << 17;  // candidate sets the side team resolves itself (else phase B)
 struct Ctrl {
   uint64_t full[kStages];   // ring slot filled
   uint64_t empty[kStages];  // ring slot drained by every consumer warp
   uint64_t cq_full[kQ], cq_empty[kQ], sq_full[kQ], sq_empty[kQ];
   ItemDesc cq[kQ], sq[kQ];
+  uint32_t side_done;       // side items finished (written by the side team)
 };
 static_assert(kCtrlOff + 2 * 3072 + sizeof(Ctrl) <= kSmemBytes, "control area");
 
@@ -1272,6 +1277,10 @@ struct Engine {
     RowState* rs = p.rs + r;
     uint32_t T = 0;
     auto pre = [&]() {
+      if (d.thr_ok) {  // read by the producer when it routed the item
+        T = d.thr;
+        return;
+      }
       if (ConsTeam::tid() == 0 && m->t_row != r) {
         uint64_t v = ld_acquire_u64(&rs->tready);
         for (uint32_t it = 0; !(v >> 32); ++it) {
@@ -1527,6 +1536,86 @@ struct Engine {
     }
   }
 
+  // Resolves a row whose matched set -- the entries of its candidate region
+  // [0, src_n) that match (prefix, plen), count of them -- is too large for
+  // smem: 12-bit histogram levels over the region (read from L2) until the
+  // matched set fits in smem or equals krem, then one pass that emits the
+  // better entries and gathers the matched ones into smem to resolve there.
+  __device__ void side_cand_resolve(int r, const RowCtx& rc, int src_n, uint64_t prefix, int plen, int krem,
+                                    int count) {
+    RowState* rs = p.rs + r;
+    const uint64_t* cand = p.cand + rc.cand_off;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kResolveHistOff);
+    uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
+    const int W = K::KB + rc.IB;
+    const int iters = (src_n + SideTeam::kSize - 1) / SideTeam::kSize;
+    auto for_entries = [&](auto&& fn) {
+      for (int it = 0; it < iters; ++it) {
+        const int i = it * SideTeam::kSize + SideTeam::tid();
+        const bool ok = i < src_n;
+        const uint64_t e = ok ? ld_cg_u64(cand + i) : 0ull;
+        const uint32_t bits = (uint32_t)(e >> 32);
+        const int64_t pos = (int64_t)(uint32_t)e;
+        const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+        fn(bits, pos, c, ok);
+      }
+    };
+    for (int guard = 0; guard < 8 && count != krem && count > kCapSB && plen < W; ++guard) {
+      const int D = min(12, W - plen);
+      const int NB = 1 << D;
+      for (int i = SideTeam::tid(); i < NB; i += SideTeam::kSize) hist[i] = 0;
+      SideTeam::sync();
+      const int sh = W - plen, sd = W - plen - D;
+      const uint32_t dm = (uint32_t)NB - 1u;
+      for_entries([&](uint32_t, int64_t, uint64_t c, bool ok) {
+        hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
+      });
+      SideTeam::sync();
+      block_select<SideTeam, false>(hist, NB, (uint32_t)krem, m);
+      if (!m->sel_found) {
+        if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
+        return;
+      }
+      prefix = (prefix << D) | m->sel_bin;
+      plen += D;
+      krem -= (int)m->sel_cum;
+      count = (int)m->sel_cnt;
+      SideTeam::sync();
+    }
+    if (count != krem && count > kCapSB) {
+      if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusLevels);
+      return;
+    }
+    const bool final_mode = count == krem;
+    const int sh = W - plen;
+    uint32_t* out_ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
+    if (SideTeam::tid() == 0) m->counter = 0;
+    SideTeam::sync();
+    for_entries([&](uint32_t bits, int64_t pos, uint64_t c, bool ok) {
+      const uint64_t t = shr64(c, sh);
+      const bool to_out = ok && (t < prefix || (final_mode && t == prefix));
+      const bool to_ent = ok && !final_mode && t == prefix;
+      if (!__any_sync(kFull, to_out || to_ent)) return;
+      const uint32_t so = warp_reserve(to_out ? 1u : 0u, out_ctr);
+      if (to_out && so < (uint32_t)rc.k) write_out<VT>(p, rc.out_off + so, bits, pos);
+      const uint32_t se = warp_reserve(to_ent ? 1u : 0u, &m->counter);
+      if (to_ent && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
+    });
+    SideTeam::sync();
+    if (!final_mode) {
+      const int ne = min((int)m->counter, kCapSB);
+      auto get = [&](int i, uint32_t& bits, int64_t& pos) {
+        const uint64_t e = ent[i];
+        bits = (uint32_t)(e >> 32);
+        pos = (int64_t)(uint32_t)e;
+      };
+      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne,
+                                        reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m, &p.hdr->status);
+      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+    }
+    post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+  }
+
   // Finisher work of a large row (all of its items are done).
   __device__ void finish_row(int r) {
     const RowCtx rc = load_row<VT, SCALE>(p, r);
@@ -1559,6 +1648,8 @@ struct Engine {
                                 &p.hdr->status);
         smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
         post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+      } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax)) {
+        side_cand_resolve(r, rc, c, 0, 0, rc.k, c);
       } else if (c >= rc.k && c <= rc.cand_cap) {
         to_phase_b(r, 1, c, 0, 0, rc.k, c);
       } else {
@@ -1578,7 +1669,9 @@ struct Engine {
       smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
       post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
     } else if (mode == kModeCand) {
-      to_phase_b(r, 1, min(m->st_candn, rc.cand_cap), m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+      const int src_n = min(m->st_candn, rc.cand_cap);
+      if (src_n <= kSideCandMax) side_cand_resolve(r, rc, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+      else to_phase_b(r, 1, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeDefer) {
       to_phase_b(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeFinal || mode == kModeAll) {
@@ -1860,7 +1953,8 @@ __device__ __forceinline__ bool is_streaming(int kind, int isA, int fin) {
 // the consumer queue and the rest to the side queue, and issues the bulk
 // copies of each streaming chunk into the ring as slots drain.
 template <int VT, bool SCALE>
-__device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, int lag, int una, int unc, int ufin) {
+__device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, int lag, int una, int unc, int ufin,
+                              int fin_tail) {
   constexpr int ES = KT<VT, SCALE>::ES, VEC = KT<VT, SCALE>::VEC;
   const int NQ = NA + NB;
   uint32_t g = 0, ci = 0, si = 0;
@@ -1880,8 +1974,22 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     mbar_arrive(&full[slot]);
     ++i;
   };
+  // In the tail of FIN items a claim is made only once this CTA's side team
+  // has finished what it holds, so the last finishes spread over the CTAs.
+  auto throttle = [&](int last_q) {
+    if (fin_tail > 0 && last_q + 1 >= NQ - fin_tail) {
+      uint32_t it = 0;
+      while (*reinterpret_cast<volatile uint32_t*>(&ctl->side_done) < si) {
+        if (++it > p.spin_limit) {
+          atomicOr(&p.hdr->status, kStatusTimeout);
+          break;
+        }
+        __nanosleep(256);
+      }
+    }
+  };
+  int q = (int)atomicAdd(&p.hdr->qhead, 1u);
   while (true) {
-    const int q = (int)atomicAdd(&p.hdr->qhead, 1u);
     ItemDesc d{};
     if (q >= NQ) {
       d.q = -1;
@@ -1898,7 +2006,14 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     d.sub = ir.isA ? ir.sub - rc.a0 : (p.uniform ? ir.sub : ir.sub - rc.b0);
     if (!is_streaming(rc.kind, ir.isA, ir.fin)) {
       push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
+      throttle(q);
+      q = (int)atomicAdd(&p.hdr->qhead, 1u);
       continue;
+    }
+    if (!ir.isA && rc.kind == kKindGridPref) {
+      const uint64_t v = ld_acquire_u64(&p.rs[ir.row].tready);
+      d.thr = (uint32_t)v;
+      d.thr_ok = (int32_t)(v >> 32);
     }
     // chunk geometry: the aligned middle goes through the ring
     const int64_t a = (int64_t)d.sub * rc.ch, b = min((int64_t)rc.n, a + rc.ch);
@@ -1917,6 +2032,11 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     d.nst = (int32_t)((nvec + kStageVecs - 1) / kStageVecs);
     d.g0 = g;
     push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
+    // Claim the next item now, so the claim's latency overlaps this chunk's
+    // copies -- except next to the FIN tail, where the claim may wait for the
+    // side team, which may need this chunk: there it follows the copies.
+    const bool near_tail = fin_tail > 0 && q + 1 >= NQ - fin_tail;
+    int nq = near_tail ? -1 : (int)atomicAdd(&p.hdr->qhead, 1u);
     const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
     uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
     for (int i = 0; i < d.nst; ++i, ++g) {
@@ -1936,6 +2056,11 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       mbar_expect_tx(&ctl->full[slot], bytes);
       bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &ctl->full[slot]);
     }
+    if (near_tail) {
+      throttle(q);
+      nq = (int)atomicAdd(&p.hdr->qhead, 1u);
+    }
+    q = nq;
   }
 }
 
@@ -1975,13 +2100,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
       mbar_init(&ctl->sq_empty[i], 1);
     }
     mbar_fence_init();
+    ctl->side_done = 0;
     for (Misc* mm : {cons_misc(smem), side_misc(smem)}) {
       mm->rel_row = -1;
       mm->t_row = -1;
     }
   }
   __syncthreads();
-  int NA, NB, lag;
+  int NA, NB, lag, fin_tail;
   int una = 1, unc = 0, ufin = 0;
   if (p.uniform) {
     const int kind = row_kind(p.u_n, p.u_k);
@@ -1991,23 +2117,31 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     NA = p.B * una;
     NB = p.B * (unc + ufin);
     lag = p.lag;
+    fin_tail = ufin ? min(p.fin_delay, p.B) : 0;
   } else {
     NA = __ldcg(&p.hdr->na);
     NB = __ldcg(&p.hdr->nb);
     lag = __ldcg(&p.hdr->lag);
+    fin_tail = __ldcg(&p.hdr->fin_tail);
   }
   const int warp = threadIdx.x >> 5;
   if (warp == kProducerWarp) {
-    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin);
+    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin, fin_tail);
   } else if (warp < kConsWarps) {
     // consumer team: streaming items
     Engine<VT, SCALE> e(p, smem, smem + kConsAreaOff, cons_misc(smem));
     Misc* m = e.m;
+    const bool releaser = ConsTeam::tid() == ConsTeam::kSize - 32;
     for (uint32_t i = 0;; ++i) {
+      // The previous item's chunk counter is released during the next item
+      // when one is already queued (its fence then overlaps that item's
+      // data); with nothing queued it is released before waiting, so no
+      // release is ever held by an idle team.
+      if (releaser) {
+        e.pending_rel = m->rel_row;
+        if (e.pending_rel >= 0 && !mbar_try_wait(&ctl->cq_full[i % kQ], (i / kQ) & 1u)) e.do_release();
+      }
       const ItemDesc d = pop_item<ConsTeam>(ctl->cq_full, ctl->cq_empty, ctl->cq, i, p);
-      // the previous item's chunk counter is released during this one
-      e.pending_rel = m->rel_row;
-      ConsTeam::sync();
       if (ConsTeam::tid() == 0) m->rel_row = -1;
       if (d.q < 0) break;
       const RowCtx rc = load_row<VT, SCALE>(p, d.row);
@@ -2040,6 +2174,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
         e.fin_item(d.row, rc);
       }
       SideTeam::sync();
+      if (SideTeam::tid() == 0) *reinterpret_cast<volatile uint32_t*>(&ctl->side_done) = i + 1;
     }
   }
   __syncthreads();

@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (threadIdx.x == 0) {
     hdr->na = (int32_t)run[0];
     hdr->nb = (int32_t)nb_total;
+    hdr->fin_tail = (int32_t)tail;
     hdr->cand_total = run[2];
     hdr->sort_total = run[3];
     hdr->plan_error = ok ? 0 : 1;

@@ -97,6 +97,36 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
  * device_bits (nullable) receives the raw device status word. */
 int radik_get_status(void* workspace, void* stream, int* device_bits);
 
+/* Size of the fixed device scratch behind radik_topk_static(). */
+#define RADIK_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
+
+/* No counterpart in RadiK.  radik_topk() for callers that may not allocate
+ * device memory at the call site: a custom allocator's own eviction or
+ * defragmentation pass that ranks blocks (calling cudaMalloc there re-enters
+ * the allocator), a hook that runs while the allocator reports out-of-memory,
+ * or a latency-bound loop where cudaFree's implicit device synchronisation is
+ * not acceptable.  The workspace is a RADIK_STATIC_SCRATCH_BYTES array of
+ * static device memory in this library, one per device, allocated when the
+ * library's device code is loaded on that device; this function allocates
+ * nothing and calls no allocating routine.
+ *   - Arguments and results as radik_topk() without workspace/workspace_bytes.
+ *   - The first call on a device looks the array up (cudaGetSymbolAddress),
+ *     which may load the library's device code; make that first call before
+ *     any stream capture on the device.
+ *   - A call whose workspace need exceeds the array fails with
+ *     RADIK_EWORKSPACE before touching the device; radik_last_error() states
+ *     the need.  Use radik_topk() with a caller-owned workspace for it.
+ *   - Nothing has to start at zero: each call clears the state it needs at
+ *     the front of the array (one memset on the stream) before its kernels.
+ *   - One array per device: two calls that can be in flight at the same time
+ *     on one device (different streams, or host threads without ordering)
+ *     race on it and corrupt each other's results.  Calls ordered on one
+ *     stream are safe.
+ *   - scratch (nullable) receives the array's device address, so that
+ *     radik_get_status(*scratch, stream, ...) reads the call's device status. */
+int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                      void* idx_out, const int* task_len, int task_num, int K, void* stream, void** scratch);
+
 /* Human-readable text of a radik_status code. */
 const char* radik_strerror(int status);
 

@@ -64,13 +64,15 @@ def lib() -> ctypes.CDLL:
     L.radik_topk.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp]
     L.radik_topk_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp]
     L.radik_get_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
+    L.radik_topk_static.argtypes = [i32, u32, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
+                                    ctypes.POINTER(vp)]
     L.radik_strerror.argtypes = [i32]
     L.radik_strerror.restype = ctypes.c_char_p
     L.radik_last_error.argtypes = []
     L.radik_last_error.restype = ctypes.c_char_p
     L.radik_version.argtypes = []
     for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
-                 "radik_get_status", "radik_version"):
+                 "radik_get_status", "radik_version", "radik_topk_static"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -235,3 +237,43 @@ def topk_rows(values, rows, *, largest: bool = True, sorted: bool = False, ascen
     if check:
         status(workspace, stream)
     return vals[:total_out], idx[:total_out]
+
+
+STATIC_SCRATCH_BYTES = 32 << 20
+
+
+def topk_static(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bool = True,
+                sorted: bool = False, ascend: Optional[bool] = None, with_scale: bool = False, idx_in=None,
+                idx64: bool = False, out=None, stream=None, check: bool = True):
+    """radik_topk_static: topk() on the library's fixed 32 MiB device scratch.
+
+    The C call allocates nothing; pass ``out=(vals, idx)`` (tensors of B*k
+    slots) to keep this wrapper allocation-free too.  Calls that need more
+    scratch raise RadikError(EWORKSPACE).  Calls in flight at the same time
+    on one device share the scratch and must not overlap.
+    """
+    import torch
+
+    if values.dim() == 2:
+        B, n = values.shape
+        lengths = [n] * B
+        flat = values.contiguous().view(-1)
+    else:
+        if lengths is None:
+            lengths = [values.numel()]
+        flat = values.contiguous()
+        B = len(lengths)
+    flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
+    if out is None:
+        out = (torch.empty((B, k), dtype=values.dtype, device=values.device),
+               torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device))
+    vals, idx = out
+    arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
+    scratch = ctypes.c_void_p(0)
+    _check(lib().radik_topk_static(dtype_code(values.dtype), flags, flat.data_ptr(),
+                                   idx_in.data_ptr() if idx_in is not None else None, vals.data_ptr(),
+                                   idx.data_ptr(), arr, B, int(k), _stream_handle(stream), ctypes.byref(scratch)))
+    if check and scratch.value:
+        bits = ctypes.c_int(0)
+        _check(lib().radik_get_status(scratch, _stream_handle(stream), ctypes.byref(bits)))
+    return vals, idx

@@ -214,6 +214,10 @@ int64_t lag_floor(bool has_radix, int grid) { return has_radix ? 2 * (int64_t)gr
 constexpr int kFinDelayRows = 64;
 int fin_delay_uniform(int nc, int grid) { return std::max(1, (3 * grid + 2 * std::max(nc, 1) - 1) / (2 * std::max(nc, 1))); }
 
+// Workspace of radik_topk_static(): static device memory of this module, one
+// copy per device the module is loaded on.
+static __device__ __align__(256) unsigned char g_static_scratch[RADIK_STATIC_SCRATCH_BYTES];
+
 }  // namespace
 }  // namespace radik
 
@@ -400,6 +404,30 @@ int radik_get_status(void* workspace, void* stream_, int* device_bits) {
   if (bits & kStatusTimeout) return fail(RADIK_ETIMEOUT, "radik: a device wait timed out");
   if (bits) return fail(RADIK_EINTERNAL, "radik: internal selection error");
   return RADIK_OK;
+}
+
+int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                      void* idx_out, const int* task_len, int task_num, int K, void* stream, void** scratch) {
+  if (scratch) *scratch = nullptr;
+  void* ws = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ws, g_static_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+  if (scratch) *scratch = ws;
+  const int rc = radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, ws, RADIK_STATIC_SCRATCH_BYTES, task_len,
+                            task_num, K, stream);
+  // ws is non-null and aligned, so RADIK_EWORKSPACE can only mean too small
+  if (rc == RADIK_EWORKSPACE) {
+    int n_max = 0;
+    for (int i = 0; i < task_num; ++i) n_max = std::max(n_max, task_len[i]);
+    size_t need = 0;
+    radik_get_workspace_size(dtype, flags, K, n_max, task_num, &need);
+    return fail(RADIK_EWORKSPACE, "radik_topk_static: " + std::to_string(task_num) + " rows of up to " +
+                                      std::to_string(n_max) + " values with K = " + std::to_string(K) +
+                                      " need up to " + std::to_string(need) + " bytes of scratch, more than the " +
+                                      std::to_string(RADIK_STATIC_SCRATCH_BYTES) +
+                                      "-byte static array; call radik_topk with a caller-owned workspace");
+  }
+  return rc;
 }
 
 }  // extern "C"

@@ -273,13 +273,13 @@ __host__ __device__ inline int32_t row_cand_cap(int kind, int32_t n) {
   return (kind == kKindGridPref || kind == kKindGridRadix) ? cand_capacity(n) : 0;
 }
 __host__ __device__ inline bool row_uses_hist(int kind) { return kind == kKindGridRadix; }
-// Pre-filter sample size (a power of two near n / 256, clamped) and the rank
+// Pre-filter sample size (a power of two near n / 128, clamped) and the rank
 // of the sampled key used as the threshold: about twice the expected rank of
 // the k-th key in the sample plus a margin of 8, so that fewer than k keys
 // pass only with negligible probability for i.i.d. rows.
 __host__ __device__ inline int32_t sample_size(int32_t n) {
   int32_t s = kSampleMin;
-  while (s < kSampleMax && (int64_t)s * 2 * 256 <= n) s *= 2;
+  while (s < kSampleMax && (int64_t)s * 2 * 128 <= n) s *= 2;
   return s;
 }
 __host__ __device__ inline int32_t sample_rank(int32_t n, int32_t k, int32_t S) {

@@ -125,6 +125,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Orders this thread's earlier generic-proxy smem accesses before later
 // async-proxy (bulk copy) writes to the same smem.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 16-byte asynchronous copy global -> smem (no registers held while in flight).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 // Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
 // global to this CTA's smem; completion is counted on `bar`.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -213,6 +218,7 @@ constexpr int kHistOff = 0;                             // first-digit histogram
 constexpr int kResolveHistOff = kCapSB * 8;             // 4096-bin histogram behind a finisher's entries
 constexpr int kSmemRowHistOff = kSmemRowCap * 4;        // behind an smem row's values
 constexpr int kSampleHistOff = kSampleMax * 4;          // behind the sampled keys
+constexpr int kSampleRawOff = kSampleHistOff + 16384;   // 16-bit sampled values before conversion
 static_assert(24 * kSinkPf * 8 <= kConsAreaBytes, "pre-filter staging");
 static_assert(24 * (kSinkCand + kSinkOut) * 8 <= kConsAreaBytes, "filter staging");
 static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B staging");
@@ -221,6 +227,7 @@ static_assert(kResolveHistOff + 16384 <= kSideAreaBytes, "finisher area");
 static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
 static_assert(32 * 128 * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert(kSampleHistOff + 16384 <= kSideAreaBytes, "sample area");
+static_assert(kSampleRawOff + kSampleMax * 2 <= kSideAreaBytes, "16-bit sample staging");
 
 struct Misc {
   uint32_t hist256[256];
@@ -666,33 +673,71 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
 // skipped (min/max reduction); then at most two 12-bit digits refine it.
 // When bits remain after that, the upper edge of the r-th key's bin is
 // returned (at least r keys are <= it).  hist: 4096 counters of smem.
+// Threshold of a pre-filter row from its sampled keys: an upper bound of the
+// r-th smallest of the cnt keys (each thread passes the min / max of the keys
+// it stored).  Past the bits all keys share, 8-bit digit levels narrow the
+// bin holding the r-th key until it holds at most 8 keys; the bin's upper end
+// is returned, so at least r sampled keys are <= the result.  256-bin levels
+// keep the clearing and the bin search to a few instructions per thread.
 template <class Tm, int KB>
-__device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r, uint32_t* hist, Misc* m,
-                                           int32_t* status) {
-  uint64_t lo = ~0ull, hi = 0;
-  for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
-    lo = min(lo, (uint64_t)keys[i]);
-    hi = max(hi, (uint64_t)keys[i]);
-  }
+__device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r, uint64_t lo, uint64_t hi,
+                                           uint32_t* hist, Misc* m, int32_t* status) {
   uint64_t mn, mx;
   block_minmax<Tm>(lo, hi, &mn, &mx, m);
   if (mn >= mx) return (uint32_t)mn;
   int plen = __clzll((long long)(mn ^ mx)) - (64 - KB);  // shared leading bits
   uint32_t prefix = plen > 0 ? (uint32_t)(mn >> (KB - plen)) : 0u;
   uint32_t krem = (uint32_t)r;
-  for (int level = 0; level < 2 && plen < KB; ++level) {
-    const int D = min(12, KB - plen);
+  while (plen < KB) {
+    const int D = min(8, KB - plen);
     const int NB = 1 << D;
-    for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+    for (int i = Tm::tid(); i < 256; i += Tm::kSize) hist[i] = 0;
+    if (Tm::tid() == 0) m->sel_found = 0;
     Tm::sync();
     const int sd = KB - plen - D;
-    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
-      const uint32_t k = keys[i];
-      const bool match = plen == 0 || (k >> (KB - plen)) == prefix;
-      if (match) atomicAdd(&hist[(k >> sd) & (uint32_t)(NB - 1)], 1u);
+    for (int b = 0; b < cnt; b += 4 * Tm::kSize) {  // four keys a thread in flight
+      uint32_t k[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = b + u * Tm::kSize + Tm::tid();
+        k[u] = i < cnt ? keys[i] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = b + u * Tm::kSize + Tm::tid();
+        if (i < cnt && (plen == 0 || (k[u] >> (KB - plen)) == prefix)) atomicAdd(&hist[(k[u] >> sd) & (uint32_t)(NB - 1)], 1u);
+      }
     }
     Tm::sync();
-    block_select<Tm, false>(hist, NB, krem, m);
+    if (Tm::wid() == 0) {  // one warp finds the bin: 8 bins a lane, then a warp scan
+      const int lane = threadIdx.x & 31;
+      uint32_t c[8], s = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        c[j] = hist[lane * 8 + j];
+        s += c[j];
+      }
+      uint32_t incl = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t run = incl - s;
+      if (run < krem && krem <= incl) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (run + c[j] >= krem && run < krem) {
+            m->sel_bin = (uint32_t)(lane * 8 + j);
+            m->sel_cum = run;
+            m->sel_cnt = c[j];
+            m->sel_found = 1;
+          }
+          run += c[j];
+        }
+      }
+    }
+    Tm::sync();
     if (!m->sel_found) {
       if (Tm::tid() == 0) atomicOr(status, kStatusSelect);
       return (uint32_t)(((uint64_t)1 << KB) - 1);
@@ -700,10 +745,34 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
     prefix = (prefix << D) | m->sel_bin;
     plen += D;
     krem -= m->sel_cum;
+    const uint32_t cnt_bin = m->sel_cnt;
     Tm::sync();
+    if (cnt_bin <= 8) break;
   }
   if (plen >= KB) return prefix;
   return (uint32_t)(((uint64_t)prefix << (KB - plen)) | (((uint64_t)1 << (KB - plen)) - 1));
+}
+
+// Copies cnt 64-bit entries from global memory (L2) into smem.  Each thread
+// issues eight loads before its first store: a plain copy loop would wait a
+// full memory round trip per element, because the compiler cannot move a
+// load above a store it cannot prove disjoint.
+template <class Tm>
+__device__ __forceinline__ void load_entries(uint64_t* dst, const uint64_t* src, int cnt) {
+  constexpr int U = 8;
+  for (int b = 0; b < cnt; b += Tm::kSize * U) {
+    uint64_t v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = b + u * Tm::kSize + Tm::tid();
+      v[u] = i < cnt ? ld_cg_u64(src + i) : 0ull;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = b + u * Tm::kSize + Tm::tid();
+      if (i < cnt) dst[i] = v[u];
+    }
+  }
 }
 
 // Entries get(i) -> (bits, pos), all matching (prefix, plen).  Refines the
@@ -750,12 +819,13 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
     const int sh = W - plen;
     const int sd = W - plen - D;
     const uint32_t dm = (uint32_t)NB - 1u;
-    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
-      uint32_t bits;
-      int64_t pos;
-      get(i, bits, pos);
+    for (int b = 0; b < cnt; b += Tm::kSize) {  // warp-uniform trip count
+      const int i = b + Tm::tid();
+      uint32_t bits = 0;
+      int64_t pos = 0;
+      if (i < cnt) get(i, bits, pos);
       const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
-      if (shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
+      if (i < cnt && shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
     }
     Tm::sync();
     block_select<Tm, false>(hist, NB, (uint32_t)krem, m);
@@ -1017,11 +1087,14 @@ struct Engine {
       if (head > 0) fe(bh, d.a + t, vh);
       if (tail > 0) fe(bt, vb + t, vt);
     }
-    const uint4* ring = reinterpret_cast<const uint4*>(base);
+    // Stage loop.  Full stages (all but a ragged last one) take no bounds
+    // checks; the slot and its phase parity advance without divisions.
+    constexpr int kPer = kStageVecs / ConsTeam::kSize;
+    const uint4* ring = reinterpret_cast<const uint4*>(base) + ConsTeam::tid();
+    uint32_t slot = d.g0 % kStages, parity = (d.g0 / kStages) & 1u;
+    const int nfull = (int)(d.nvec / kStageVecs);
+    int64_t pos = d.va + (int64_t)ConsTeam::tid() * VEC;  // first element of this thread's vector in the stage
     for (int i = 0; i < d.nst; ++i) {
-      const uint32_t g = d.g0 + (uint32_t)i;
-      const uint32_t slot = g % kStages;
-      const uint32_t parity = (g / kStages) & 1u;
       uint32_t it = 0;
       while (!mbar_try_wait(&ctl->full[slot], parity)) {
         if (++it > p.spin_limit) {
@@ -1029,18 +1102,26 @@ struct Engine {
           break;
         }
       }
-      const int64_t v0 = (int64_t)i * kStageVecs;
-      const int cnt = (int)min((int64_t)kStageVecs, d.nvec - v0);
-      const uint4* st = ring + (size_t)slot * kStageVecs;
+      const uint4* st = ring + slot * kStageVecs;
+      if (i < nfull) {
 #pragma unroll
-      for (int j = 0; j < kStageVecs / ConsTeam::kSize; ++j) {
-        const int v = j * ConsTeam::kSize + ConsTeam::tid();
-        const bool ok = v < cnt;
-        const uint4 x = ok ? st[v] : make_uint4(0, 0, 0, 0);
-        fv(x, d.va + (v0 + v) * VEC, ok);
+        for (int j = 0; j < kPer; ++j) fv(st[j * ConsTeam::kSize], pos + (int64_t)j * ConsTeam::kSize * VEC, true);
+      } else {
+        const int cnt = (int)(d.nvec - (int64_t)i * kStageVecs);
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+          const bool ok = j * ConsTeam::kSize + ConsTeam::tid() < cnt;
+          const uint4 x = ok ? st[j * ConsTeam::kSize] : make_uint4(0, 0, 0, 0);
+          fv(x, pos + (int64_t)j * ConsTeam::kSize * VEC, ok);
+        }
       }
+      pos += (int64_t)kStageVecs * VEC;
       __syncwarp();
       if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
+      if (++slot == (uint32_t)kStages) {
+        slot = 0;
+        parity ^= 1u;
+      }
     }
   }
 
@@ -1064,21 +1145,41 @@ struct Engine {
   }
 
   // ---- threshold from a strided sample of the row (one CTA).
-  // The sample is S keys in sectors of 32 bytes spread evenly over the row.
+  // The sample is S keys in nsec = S / (32 / ES) whole 32-byte sectors spread
+  // evenly over the row's aligned sectors (pre-filter rows hold more than 2^18
+  // keys, far more sectors than the sample needs).  All sectors are fetched by
+  // asynchronous copies into smem at once, so the sample costs about one
+  // memory round trip and holds no registers while in flight.
   __device__ uint32_t sample_threshold(const RowCtx& rc) {
     uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
     const int S = sample_size(rc.n);
-    constexpr int SE = 32 / ES;  // elements per sector
+    constexpr int SE = 32 / ES;  // keys per sector
     const int nsec = S / SE;
-    const int64_t span = (int64_t)rc.n - SE;
-    for (int j = SideTeam::tid(); j < S; j += SideTeam::kSize) {
-      const int i = j / SE, o = j % SE;
-      const int64_t pos = (nsec > 1 ? (int64_t)i * span / (nsec - 1) : 0) + o;
-      keys[j] = key_of(load_bits(rc, pos), rc);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p.val_in) + (uintptr_t)rc.in_off * ES;
+    const int64_t first = (int64_t)((a + 31) / 32);
+    const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 32) - first;  // whole sectors in the row
+    // fp32 values are converted to keys in place; 16-bit values are staged apart
+    uint8_t* raw = ES == 4 ? smem : smem + kSampleRawOff;
+    for (int j = SideTeam::tid(); j < 2 * nsec; j += SideTeam::kSize) {
+      const int i = j >> 1;
+      const int64_t sec = first + (nsec > 1 ? (int64_t)i * (nfull - 1) / (nsec - 1) : 0);
+      cp_async16(raw + (size_t)j * 16, reinterpret_cast<const void*>((uintptr_t)sec * 32 + (uintptr_t)(j & 1) * 16));
+    }
+    cp_async_wait_all();
+    SideTeam::sync();
+    uint64_t lo = ~0ull, hi = 0;
+    for (int i = SideTeam::tid(); i < S; i += SideTeam::kSize) {
+      const uint32_t bits = ES == 4 ? reinterpret_cast<const uint32_t*>(raw)[i]
+                                    : (uint32_t)reinterpret_cast<const unsigned short*>(raw)[i];
+      const uint32_t k = key_of(bits, rc);
+      keys[i] = k;
+      lo = min(lo, (uint64_t)k);
+      hi = max(hi, (uint64_t)k);
     }
     SideTeam::sync();
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
-    const uint32_t t = block_sample_threshold<SideTeam, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), hist, m, &p.hdr->status);
+    const uint32_t t = block_sample_threshold<SideTeam, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,
+                                                               &p.hdr->status);
     SideTeam::sync();
     return t;
   }
@@ -1309,6 +1410,27 @@ struct Engine {
     auto push = [&](uint32_t hm, uint32_t e0bits_unused, auto elem_bits, int64_t pos0) {
       (void)e0bits_unused;
       const uint32_t h = (uint32_t)__popc(hm);
+      // Usual case: a single lane holds all of the warp's hits.
+      const unsigned lanes = __ballot_sync(kFull, hm != 0u);
+      if (__popc(lanes) == 1) {
+        const int src = __ffs(lanes) - 1;
+        const uint32_t tot = __shfl_sync(kFull, h, src);
+        if (cb.n + tot > (uint32_t)kCap) {
+          __syncwarp();
+          flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+          cb.n = 0;
+          __syncwarp();
+        }
+        if ((int)lane == src) {
+          uint32_t w = cb.n;
+          for (uint32_t mm = hm; mm; mm &= mm - 1) {
+            const int e = __ffs(mm) - 1;
+            cb.buf[w++] = make_entry(elem_bits(e), pos0 + e);
+          }
+        }
+        cb.n += tot;
+        return;
+      }
       uint32_t x = h;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -1548,16 +1670,25 @@ struct Engine {
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kResolveHistOff);
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
     const int W = K::KB + rc.IB;
-    const int iters = (src_n + SideTeam::kSize - 1) / SideTeam::kSize;
+    // entries in groups of four per thread, loaded before they are used
+    constexpr int U = 4;
+    const int iters = (src_n + SideTeam::kSize * U - 1) / (SideTeam::kSize * U);
     auto for_entries = [&](auto&& fn) {
       for (int it = 0; it < iters; ++it) {
-        const int i = it * SideTeam::kSize + SideTeam::tid();
-        const bool ok = i < src_n;
-        const uint64_t e = ok ? ld_cg_u64(cand + i) : 0ull;
-        const uint32_t bits = (uint32_t)(e >> 32);
-        const int64_t pos = (int64_t)(uint32_t)e;
-        const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
-        fn(bits, pos, c, ok);
+        uint64_t e[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int i = (it * U + u) * SideTeam::kSize + SideTeam::tid();
+          e[u] = i < src_n ? ld_cg_u64(cand + i) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int i = (it * U + u) * SideTeam::kSize + SideTeam::tid();
+          const uint32_t bits = (uint32_t)(e[u] >> 32);
+          const int64_t pos = (int64_t)(uint32_t)e[u];
+          const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
+          fn(bits, pos, c, i < src_n);
+        }
       }
     };
     for (int guard = 0; guard < 8 && count != krem && count > kCapSB && plen < W; ++guard) {
@@ -1640,7 +1771,7 @@ struct Engine {
     if (rc.kind == kKindGridPref) {
       const int c = m->st_candn;
       if (c >= rc.k && c <= kCapSB) {
-        for (int i = SideTeam::tid(); i < c; i += SideTeam::kSize) ent[i] = ld_cg_u64(cand + i);
+        load_entries<SideTeam>(ent, cand, c);
         SideTeam::sync();
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
@@ -1660,7 +1791,7 @@ struct Engine {
     const int mode = m->st_mode;
     if (mode == kModeSB) {
       const int ne = min(m->st_candn, kCapSB);
-      for (int i = SideTeam::tid(); i < ne; i += SideTeam::kSize) ent[i] = ld_cg_u64(cand + i);
+      load_entries<SideTeam>(ent, cand, ne);
       uint64_t prefix = m->st_prefix;
       int plen = m->st_plen, krem = m->st_krem;
       SideTeam::sync();
@@ -1859,7 +1990,7 @@ struct Engine {
         if (count != krem0) {
           const int ne = min(__ldcg(&rs->sb_count), kCapSB);
           const uint64_t* sb = p.pb_sb + (size_t)i * kCapSB;
-          for (int j = FullTeam::tid(); j < ne; j += FullTeam::kSize) ent[j] = ld_cg_u64(sb + j);
+          load_entries<FullTeam>(ent, sb, ne);
           uint64_t prefix = ld_cg_u64(&rs->prefix);
           int plen = __ldcg(&rs->plen), krem = krem0;
           FullTeam::sync();
@@ -2011,7 +2142,15 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       continue;
     }
     if (!ir.isA && rc.kind == kKindGridPref) {
-      const uint64_t v = ld_acquire_u64(&p.rs[ir.row].tready);
+      // The chunk is useless before its row's threshold exists, so its copies
+      // wait for it: at the start this keeps the ring fills of all CTAs from
+      // queueing ahead of the sample reads that produce the thresholds.  The
+      // sample item precedes the chunk in the claim order, so the wait ends.
+      uint64_t v = ld_acquire_u64(&p.rs[ir.row].tready);
+      for (uint32_t it = 0; !(v >> 32) && it < p.spin_limit; ++it) {
+        __nanosleep(128);
+        v = ld_acquire_u64(&p.rs[ir.row].tready);
+      }
       d.thr = (uint32_t)v;
       d.thr_ok = (int32_t)(v >> 32);
     }
@@ -2035,8 +2174,11 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     // Claim the next item now, so the claim's latency overlaps this chunk's
     // copies -- except next to the FIN tail, where the claim may wait for the
     // side team, which may need this chunk: there it follows the copies.
+    // The last grid of items is claimed only when this item's copies are all
+    // issued: a claim made early holds an item that an idle CTA could start.
     const bool near_tail = fin_tail > 0 && q + 1 >= NQ - fin_tail;
-    int nq = near_tail ? -1 : (int)atomicAdd(&p.hdr->qhead, 1u);
+    const bool late_claim = near_tail || q + 1 >= NQ - fin_tail - (int)gridDim.x;
+    int nq = late_claim ? -1 : (int)atomicAdd(&p.hdr->qhead, 1u);
     const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
     uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
     for (int i = 0; i < d.nst; ++i, ++g) {
@@ -2056,7 +2198,7 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       mbar_expect_tx(&ctl->full[slot], bytes);
       bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &ctl->full[slot]);
     }
-    if (near_tail) {
+    if (late_claim) {
       throttle(q);
       nq = (int)atomicAdd(&p.hdr->qhead, 1u);
     }

@@ -41,6 +41,15 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (read + write) per engine launch measured by ncu, for the
+# workloads whose capture is summarised under profiles/ (the 256-row figure is
+# the 64-row capture scaled by rows: traffic grows with the rows streamed).
+NCU_TRAFFIC = {
+    ("batched", 256): 4 * (274446592 + 5250048),  # profiles/engine_kernel_f32_64x1M_k256_full.md
+    ("batched", 64): 274446592 + 5250048,
+}
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -293,7 +302,8 @@ def main():
         "e2e": {"value": round(e2e_value, 3), "unit": "Gkeys/s", "h2d_bytes_per_step": keys_per_step * es,
                 "d2h_bytes_per_step": B * k * (es + 4)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": NCU_TRAFFIC.get((args.workload, B)) if args.impl != "reference" else None,
                      "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": algo_bytes,
                      "step_ms_median": round(statistics.median(step_ms), 5)},
         "clocks": clocks,

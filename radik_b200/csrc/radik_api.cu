@@ -130,9 +130,9 @@ int env_int(const char* name, int dflt) {
 }
 
 // Tunables: chunk lengths and first-digit width.  Single-read rows use
-// chunks of 4K..256K elements, aiming at about four chunks per CTA so the
-// work queue balances while each chunk streams long enough to amortise its
-// item overhead.  Radix rows use 32K-element chunks: their filter items
+// chunks of 4K..256K elements, aiming at about eight chunks per CTA so the
+// work queue balances (the last chunks bound the tail) while each chunk
+// streams long enough to amortise its item overhead.  Radix rows use 32K-element chunks: their filter items
 // re-read chunks that the histogram items read two grids earlier, and that
 // window (2 x 148 x 128 KB) must stay in L2.  The 14-bit first digit (16384
 // bins, 64 KB of smem) leaves about n/64 keys of an i.i.d. fp32 row in the
@@ -143,7 +143,7 @@ struct Config {
 
 Config choose_config(int64_t stream_elems, int grid) {
   Config c{};
-  const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 4));
+  const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 8));
   int ch = kMinCH;
   while (ch < kMaxCH && ch * 2 <= target) ch *= 2;
   c.CH = ch;

@@ -673,6 +673,44 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
 // skipped (min/max reduction); then at most two 12-bit digits refine it.
 // When bits remain after that, the upper edge of the r-th key's bin is
 // returned (at least r keys are <= it).  hist: 4096 counters of smem.
+// Finds the bin b of h[0..256) with cum(<b) < krem <= cum(<=b) using one
+// warp (8 bins a lane, then a warp scan).  Result in m->sel_*; m->sel_found
+// = 0 if the bins hold fewer than krem.  Ends with a team barrier.
+template <class Tm>
+__device__ void select256(const uint32_t* hist, uint32_t krem, Misc* m) {
+  if (Tm::wid() == 0) {
+    const int lane = threadIdx.x & 31;
+    uint32_t c[8], s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      c[j] = hist[lane * 8 + j];
+      s += c[j];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (lane == 0 && total < krem) m->sel_found = 0;
+    uint32_t run = incl - s;
+    if (run < krem && krem <= incl) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (run + c[j] >= krem && run < krem) {
+          m->sel_bin = (uint32_t)(lane * 8 + j);
+          m->sel_cum = run;
+          m->sel_cnt = c[j];
+          m->sel_found = 1;
+        }
+        run += c[j];
+      }
+    }
+  }
+  Tm::sync();
+}
+
 // Threshold of a pre-filter row from its sampled keys: an upper bound of the
 // r-th smallest of the cnt keys (each thread passes the min / max of the keys
 // it stored).  Past the bits all keys share, 8-bit digit levels narrow the
@@ -692,7 +730,6 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
     const int D = min(8, KB - plen);
     const int NB = 1 << D;
     for (int i = Tm::tid(); i < 256; i += Tm::kSize) hist[i] = 0;
-    if (Tm::tid() == 0) m->sel_found = 0;
     Tm::sync();
     const int sd = KB - plen - D;
     for (int b = 0; b < cnt; b += 4 * Tm::kSize) {  // four keys a thread in flight
@@ -709,35 +746,7 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
       }
     }
     Tm::sync();
-    if (Tm::wid() == 0) {  // one warp finds the bin: 8 bins a lane, then a warp scan
-      const int lane = threadIdx.x & 31;
-      uint32_t c[8], s = 0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        c[j] = hist[lane * 8 + j];
-        s += c[j];
-      }
-      uint32_t incl = s;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-      }
-      uint32_t run = incl - s;
-      if (run < krem && krem <= incl) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (run + c[j] >= krem && run < krem) {
-            m->sel_bin = (uint32_t)(lane * 8 + j);
-            m->sel_cum = run;
-            m->sel_cnt = c[j];
-            m->sel_found = 1;
-          }
-          run += c[j];
-        }
-      }
-    }
-    Tm::sync();
+    select256<Tm>(hist, krem, m);
     if (!m->sel_found) {
       if (Tm::tid() == 0) atomicOr(status, kStatusSelect);
       return (uint32_t)(((uint64_t)1 << KB) - 1);
@@ -812,23 +821,24 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
       if (Tm::tid() == 0) atomicOr(status, kStatusLevels);
       break;
     }
-    const int D = min(12, W - plen);
+    // 8-bit digits: the sets here are small (smem), so a level's fixed cost
+    // (clearing the bins, finding the bin) matters more than its pass count
+    const int D = min(8, W - plen);
     const int NB = 1 << D;
-    for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+    for (int i = Tm::tid(); i < 256; i += Tm::kSize) hist[i] = 0;
     Tm::sync();
     const int sh = W - plen;
     const int sd = W - plen - D;
     const uint32_t dm = (uint32_t)NB - 1u;
-    for (int b = 0; b < cnt; b += Tm::kSize) {  // warp-uniform trip count
-      const int i = b + Tm::tid();
-      uint32_t bits = 0;
-      int64_t pos = 0;
-      if (i < cnt) get(i, bits, pos);
+    for (int i = Tm::tid(); i < cnt; i += Tm::kSize) {
+      uint32_t bits;
+      int64_t pos;
+      get(i, bits, pos);
       const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
-      if (i < cnt && shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
+      if (shr64(c, sh) == prefix) atomicAdd(&hist[(uint32_t)shr64(c, sd) & dm], 1u);
     }
     Tm::sync();
-    block_select<Tm, false>(hist, NB, (uint32_t)krem, m);
+    select256<Tm>(hist, (uint32_t)krem, m);
     if (!m->sel_found) {
       if (Tm::tid() == 0) atomicOr(status, kStatusSelect);
       break;
@@ -1160,22 +1170,38 @@ struct Engine {
     const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 32) - first;  // whole sectors in the row
     // fp32 values are converted to keys in place; 16-bit values are staged apart
     uint8_t* raw = ES == 4 ? smem : smem + kSampleRawOff;
+    // sector i sits at first + floor(i * (nfull - 1) / (nsec - 1)), stepped in
+    // 32.32 fixed point (one division per thread instead of one per sector)
+    const uint64_t step = nsec > 1 ? ((uint64_t)(nfull - 1) << 32) / (uint64_t)(nsec - 1) : 0;
     for (int j = SideTeam::tid(); j < 2 * nsec; j += SideTeam::kSize) {
       const int i = j >> 1;
-      const int64_t sec = first + (nsec > 1 ? (int64_t)i * (nfull - 1) / (nsec - 1) : 0);
+      const int64_t sec = first + (int64_t)(((uint64_t)i * step) >> 32);
       cp_async16(raw + (size_t)j * 16, reinterpret_cast<const void*>((uintptr_t)sec * 32 + (uintptr_t)(j & 1) * 16));
     }
     cp_async_wait_all();
     SideTeam::sync();
-    uint64_t lo = ~0ull, hi = 0;
-    for (int i = SideTeam::tid(); i < S; i += SideTeam::kSize) {
-      const uint32_t bits = ES == 4 ? reinterpret_cast<const uint32_t*>(raw)[i]
-                                    : (uint32_t)reinterpret_cast<const unsigned short*>(raw)[i];
-      const uint32_t k = key_of(bits, rc);
-      keys[i] = k;
-      lo = min(lo, (uint64_t)k);
-      hi = max(hi, (uint64_t)k);
+    uint32_t lo32 = 0xFFFFFFFFu, hi32 = 0;
+    for (int b = 0; b < S; b += 4 * SideTeam::kSize) {  // four keys a thread in flight
+      uint32_t bits[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = b + u * SideTeam::kSize + SideTeam::tid();
+        bits[u] = i >= S ? 0u
+                         : ES == 4 ? reinterpret_cast<const uint32_t*>(raw)[i]
+                                   : (uint32_t)reinterpret_cast<const unsigned short*>(raw)[i];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = b + u * SideTeam::kSize + SideTeam::tid();
+        if (i < S) {
+          const uint32_t k = key_of(bits[u], rc);
+          keys[i] = k;
+          lo32 = min(lo32, k);
+          hi32 = max(hi32, k);
+        }
+      }
     }
+    const uint64_t lo = lo32 == 0xFFFFFFFFu && hi32 == 0 ? ~0ull : (uint64_t)lo32, hi = hi32;
     SideTeam::sync();
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
     const uint32_t t = block_sample_threshold<SideTeam, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,

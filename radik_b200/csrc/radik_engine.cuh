@@ -275,6 +275,7 @@ struct Ctrl {
   uint64_t cq_full[kQ], cq_empty[kQ], sq_full[kQ], sq_empty[kQ];
   ItemDesc cq[kQ], sq[kQ];
   uint32_t side_done;       // side items finished (written by the side team)
+  int32_t first_q;          // the CTA's first claim
 };
 static_assert(kCtrlOff + 2 * 3072 + sizeof(Ctrl) <= kSmemBytes, "control area");
 
@@ -1154,45 +1155,46 @@ struct Engine {
     else return (uint32_t)__ldg(static_cast<const unsigned short*>(p.val_in) + rc.in_off + pos);
   }
 
-  // ---- threshold from a strided sample of the row (one CTA).
-  // The sample is S keys in nsec = S / (32 / ES) whole 32-byte sectors spread
-  // evenly over the row's aligned sectors (pre-filter rows hold more than 2^18
-  // keys, far more sectors than the sample needs).  All sectors are fetched by
-  // asynchronous copies into smem at once, so the sample costs about one
+  // ---- threshold from a strided sample of the row (one team of a CTA).
+  // The sample is S keys in S / (128 / ES) whole 128-byte lines spread evenly
+  // over the row's aligned lines (pre-filter rows hold more than 2^18 keys,
+  // far more lines than the sample needs).  All lines are fetched at once by
+  // 16-byte asynchronous copies into smem, so the sample costs about one
   // memory round trip and holds no registers while in flight.
+  template <class Tm>
   __device__ uint32_t sample_threshold(const RowCtx& rc) {
     uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
     const int S = sample_size(rc.n);
-    constexpr int SE = 32 / ES;  // keys per sector
-    const int nsec = S / SE;
+    constexpr int SL = 128 / ES;  // keys per line
+    const int nlines = S / SL;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.val_in) + (uintptr_t)rc.in_off * ES;
-    const int64_t first = (int64_t)((a + 31) / 32);
-    const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 32) - first;  // whole sectors in the row
+    const int64_t first = (int64_t)((a + 127) / 128);
+    const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 128) - first;  // whole lines in the row
     // fp32 values are converted to keys in place; 16-bit values are staged apart
     uint8_t* raw = ES == 4 ? smem : smem + kSampleRawOff;
-    // sector i sits at first + floor(i * (nfull - 1) / (nsec - 1)), stepped in
-    // 32.32 fixed point (one division per thread instead of one per sector)
-    const uint64_t step = nsec > 1 ? ((uint64_t)(nfull - 1) << 32) / (uint64_t)(nsec - 1) : 0;
-    for (int j = SideTeam::tid(); j < 2 * nsec; j += SideTeam::kSize) {
-      const int i = j >> 1;
-      const int64_t sec = first + (int64_t)(((uint64_t)i * step) >> 32);
-      cp_async16(raw + (size_t)j * 16, reinterpret_cast<const void*>((uintptr_t)sec * 32 + (uintptr_t)(j & 1) * 16));
+    // line i sits at first + floor(i * (nfull - 1) / (nlines - 1)), stepped in
+    // 32.32 fixed point (one division per thread instead of one per line)
+    const uint64_t step = nlines > 1 ? ((uint64_t)(nfull - 1) << 32) / (uint64_t)(nlines - 1) : 0;
+    for (int j = Tm::tid(); j < 8 * nlines; j += Tm::kSize) {
+      const int i = j >> 3;
+      const int64_t line = first + (int64_t)(((uint64_t)i * step) >> 32);
+      cp_async16(raw + (size_t)j * 16, reinterpret_cast<const void*>((uintptr_t)line * 128 + (uintptr_t)(j & 7) * 16));
     }
     cp_async_wait_all();
-    SideTeam::sync();
+    Tm::sync();
     uint32_t lo32 = 0xFFFFFFFFu, hi32 = 0;
-    for (int b = 0; b < S; b += 4 * SideTeam::kSize) {  // four keys a thread in flight
+    for (int b = 0; b < S; b += 4 * Tm::kSize) {  // four keys a thread in flight
       uint32_t bits[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int i = b + u * SideTeam::kSize + SideTeam::tid();
+        const int i = b + u * Tm::kSize + Tm::tid();
         bits[u] = i >= S ? 0u
                          : ES == 4 ? reinterpret_cast<const uint32_t*>(raw)[i]
                                    : (uint32_t)reinterpret_cast<const unsigned short*>(raw)[i];
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int i = b + u * SideTeam::kSize + SideTeam::tid();
+        const int i = b + u * Tm::kSize + Tm::tid();
         if (i < S) {
           const uint32_t k = key_of(bits[u], rc);
           keys[i] = k;
@@ -1202,11 +1204,11 @@ struct Engine {
       }
     }
     const uint64_t lo = lo32 == 0xFFFFFFFFu && hi32 == 0 ? ~0ull : (uint64_t)lo32, hi = hi32;
-    SideTeam::sync();
+    Tm::sync();
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
-    const uint32_t t = block_sample_threshold<SideTeam, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,
-                                                               &p.hdr->status);
-    SideTeam::sync();
+    const uint32_t t = block_sample_threshold<Tm, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,
+                                                         &p.hdr->status);
+    Tm::sync();
     return t;
   }
 
@@ -1273,7 +1275,7 @@ struct Engine {
     };
     if ((int64_t)rc.k * kPrefRatio <= rc.n) {
       // pre-filter inside the CTA
-      const uint32_t T = sample_threshold(rc);
+      const uint32_t T = sample_threshold<SideTeam>(rc);
       if (SideTeam::tid() == 0) m->counter = 0;
       SideTeam::sync();
       auto one = [&](uint32_t bits, int64_t pos, bool ok) {
@@ -1389,10 +1391,12 @@ struct Engine {
   }
 
   // ---- sample item of a pre-filter row: publish the threshold
-  __device__ void sample_item(int r, const RowCtx& rc) {
-    const uint32_t T = sample_threshold(rc);
-    if (SideTeam::tid() == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
+  template <class Tm>
+  __device__ void sample_item_t(int r, const RowCtx& rc) {
+    const uint32_t T = sample_threshold<Tm>(rc);
+    if (Tm::tid() == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
   }
+  __device__ void sample_item(int r, const RowCtx& rc) { sample_item_t<SideTeam>(r, rc); }
 
   // ---- filter item of a pre-filter row: keys <= T into the candidates.
   // Hot loop: a float (or half2) compare against the threshold's value with
@@ -2111,7 +2115,7 @@ __device__ __forceinline__ bool is_streaming(int kind, int isA, int fin) {
 // copies of each streaming chunk into the ring as slots drain.
 template <int VT, bool SCALE>
 __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, int lag, int una, int unc, int ufin,
-                              int fin_tail) {
+                              int fin_tail, int first_q) {
   constexpr int ES = KT<VT, SCALE>::ES, VEC = KT<VT, SCALE>::VEC;
   const int NQ = NA + NB;
   uint32_t g = 0, ci = 0, si = 0;
@@ -2145,7 +2149,7 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       }
     }
   };
-  int q = (int)atomicAdd(&p.hdr->qhead, 1u);
+  int q = first_q >= 0 ? first_q : (int)atomicAdd(&p.hdr->qhead, 1u);
   while (true) {
     ItemDesc d{};
     if (q >= NQ) {
@@ -2292,9 +2296,24 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     lag = __ldcg(&p.hdr->lag);
     fin_tail = __ldcg(&p.hdr->fin_tail);
   }
+  // The CTA's first claim.  A pre-filter sample claimed here is computed by
+  // the whole CTA before the teams start: nothing streams until the first
+  // thresholds exist, so these samples are on every CTA's critical path.
+  if (threadIdx.x == 0) ctl->first_q = (int)atomicAdd(&p.hdr->qhead, 1u);
+  __syncthreads();
+  int first_q = ctl->first_q;
+  if (first_q < NA + NB) {
+    const ItemRef ir = resolve_item(p, first_q, NA, NB, lag, una, unc, ufin);
+    const RowCtx rc = load_row<VT, SCALE>(p, ir.row);
+    if (ir.isA && rc.kind == kKindGridPref) {
+      Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
+      e.template sample_item_t<FullTeam>(ir.row, rc);
+      first_q = -1;
+    }
+  }
   const int warp = threadIdx.x >> 5;
   if (warp == kProducerWarp) {
-    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin, fin_tail);
+    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin, fin_tail, first_q);
   } else if (warp < kConsWarps) {
     // consumer team: streaming items
     Engine<VT, SCALE> e(p, smem, smem + kConsAreaOff, cons_misc(smem));

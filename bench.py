@@ -152,13 +152,291 @@ def cpu_baseline(x: np.ndarray, B, n, k, sorted_, largest, budget_s: float):
                       f"{' + sort' if sorted_ else ''} per row on {threads} host threads"}
 
 
+def _events(n):
+    import torch
+
+    return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+
+
+def run_uneven(args, dev, world, rank):
+    """Uneven batched top-k: 4096 fp32 rows, n log-uniform in [2^10, 2^22], k
+    log-uniform in [1, min(2048, n)], N(0,1) values.  One step = one
+    radik_topk_rows launch over all rows (device descriptors, replayed from a
+    CUDA graph).  Reported beside it: the plain per-row form (one radik_topk
+    call per row, the way a RadiK caller handles rows of different k)."""
+    import ctypes
+
+    import torch
+
+    from radik_b200 import workloads
+
+    B = 4096 if args.rows <= 0 else args.rows
+    ns, ks = workloads.uneven_rows(B, 7)
+    total_n, n_max, k_max = sum(ns), max(ns), max(ks)
+    offs = np.concatenate([[0], np.cumsum(ns)[:-1]]).astype(np.int64)
+    oo = np.concatenate([[0], np.cumsum(ks)[:-1]]).astype(np.int64)
+    total_out = int(sum(ks))
+    x = np.empty(total_n, np.float32)
+    for r in range(B):
+        x[offs[r]:offs[r] + ns[r]] = workloads.normal(ns[r], 1000 + r)
+    host = torch.from_numpy(x).pin_memory()
+    dev_in = host.to(dev)
+    stream = torch.cuda.current_stream(dev)
+    desc = np.zeros(B, dtype=[("in_off", "<i8"), ("out_off", "<i8"), ("n", "<i4"), ("k", "<i4")])
+    desc["in_off"], desc["out_off"], desc["n"], desc["k"] = offs, oo, ns, ks
+    desc_dev = torch.from_numpy(desc.view(np.uint8).copy()).to(dev)
+    algo_bytes = total_n * 4 + total_out * 8
+    peak, peak_kind = load_peaks()
+    out = {"metric": "Gkeys/s & % HBM peak; uneven-batch speedup vs plain per-row; serving p50/p99",
+           "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic: N(0,1) from numpy Philox-4x32-10, row r seed 1000 + r; lengths/k seed 7",
+           "config": {"workload": f"uneven batched top-k, {B} fp32 rows, n log-uniform in [2^10, 2^22], "
+                                  f"k log-uniform in [1, min(2048, n)], largest, unsorted",
+                      "rows": B, "total_keys": total_n, "n_max": n_max, "k_max": k_max,
+                      "l2": "inputs (%d MiB) larger than L2; no flush" % (total_n * 4 >> 20),
+                      "parallelism": f"rows replicated per GPU x{world} (no collective)"}}
+    vals = torch.empty(total_out, dtype=torch.float32, device=dev)
+    idx = torch.empty(total_out, dtype=torch.int32, device=dev)
+
+    if args.impl == "reference":
+        import oracle
+
+        ref = oracle.RefRadik()
+        ws = torch.empty(ref.workspace_size(0, k_max, n_max, 1), dtype=torch.uint8, device=dev)
+
+        # The reference reads rows with 16-byte vector loads and takes the
+        # alignment of a row from its offset inside the batch, so a row pointer
+        # of its own must be 16-byte aligned: its rows sit at padded offsets.
+        offs_ref = np.zeros(B, np.int64)
+        offs_ref[1:] = np.cumsum((np.asarray(ns, np.int64) + 3) // 4 * 4)[:-1]
+        padded = torch.zeros(int(offs_ref[-1] + ns[-1] + 4), dtype=torch.float32, device=dev)
+        for r in range(B):
+            padded[int(offs_ref[r]):int(offs_ref[r]) + ns[r]] = dev_in[int(offs[r]):int(offs[r]) + ns[r]]
+
+        def step(inp):
+            base_v = padded.data_ptr()
+            for r in range(B):
+                ref.topk(0, True, False, False, False, base_v + 4 * int(offs_ref[r]), vals.data_ptr() + 4 * int(oo[r]),
+                         idx.data_ptr() + 4 * int(oo[r]), ws.data_ptr(), [ns[r]], ks[r], stream.cuda_stream)
+        launches = None
+    else:
+        import radik_b200 as rk
+
+        L = rk.lib()
+        flags = rk.make_flags(True, False)
+        ws = torch.empty(rk.get_rows_workspace_size(rk.F32, B, total_n, n_max, k_max, flags), dtype=torch.uint8,
+                         device=dev)
+
+        def call(inp):
+            rk._check(L.radik_topk_rows(rk.F32, flags, inp.data_ptr(), None, vals.data_ptr(), idx.data_ptr(),
+                                        ws.data_ptr(), ws.numel(), desc_dev.data_ptr(), B, total_n, n_max, k_max,
+                                        torch.cuda.current_stream(dev).cuda_stream))
+
+        for _ in range(args.warmup):
+            call(dev_in)
+        torch.cuda.synchronize(dev)
+        rk.status(ws, stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            call(dev_in)
+        torch.cuda.synchronize(dev)
+
+        def step(inp):
+            graph.replay()
+        launches = 2  # planning kernel + selection engine (the workspace clear is a memset node)
+        # plain per-row form: one radik_topk call per row, arguments prepared up front
+        ws_row = torch.empty(rk.get_radix_select_l_workspace_size(rk.F32, k_max, n_max, 1, flags), dtype=torch.uint8,
+                             device=dev)
+        lens = [(ctypes.c_int * 1)(n) for n in ns]
+        v0, o0, i0, w0 = dev_in.data_ptr(), vals.data_ptr(), idx.data_ptr(), ws_row.data_ptr()
+        wsz, sh = ws_row.numel(), stream.cuda_stream
+
+        def per_row():
+            for r in range(B):
+                L.radik_topk(rk.F32, flags, v0 + 4 * int(offs[r]), None, o0 + 4 * int(oo[r]), i0 + 4 * int(oo[r]),
+                             w0, wsz, lens[r], 1, ks[r], sh)
+        per_row()
+        torch.cuda.synchronize(dev)
+        ev = _events(1)[0]
+        ev[0].record(stream)
+        per_row()
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        per_row_ms = ev[0].elapsed_time(ev[1])
+        rk.status(ws_row, stream)
+
+    for _ in range(args.warmup):
+        step(dev_in)
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    evs = _events(args.steps)
+    t0, t1 = _events(1)[0]
+    t0.record(stream)
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        step(dev_in)
+        evs[i][1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = t0.elapsed_time(t1)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    vals_h = torch.empty(total_out, dtype=torch.float32).pin_memory()
+    idx_h = torch.empty(total_out, dtype=torch.int32).pin_memory()
+    e0, e1 = _events(1)[0]
+    e_steps = max(1, min(args.steps, 5))
+    e0.record(stream)
+    for i in range(e_steps):
+        dev_in.copy_(host, non_blocking=True)
+        step(dev_in)
+        vals_h.copy_(vals, non_blocking=True)
+        idx_h.copy_(idx, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1) / e_steps
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+    ms = total_ms / args.steps
+    out["value"] = round(world * total_n / (ms / 1e3) / 1e9, 3)
+    out["ms_per_step"] = round(ms, 5)
+    out["e2e"] = {"value": round(world * total_n / (e2e_ms / 1e3) / 1e9, 3), "unit": "Gkeys/s",
+                  "h2d_bytes_per_step": total_n * 4, "d2h_bytes_per_step": total_out * 8}
+    achieved = algo_bytes / (statistics.mean(step_ms) / 1e3) / 1e9
+    out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(achieved / peak, 4), "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
+                       "algorithmic_bytes_per_launch": algo_bytes}
+    out["clocks"] = clocks
+    if args.impl == "reference":
+        out["impl"] = "reference"
+        out["gpu_launches"] = None
+        out["cpu_baseline"] = {"value": out["value"], "unit": "Gkeys/s", "cores": 1, "kind": "reference",
+                               "sample": "the reference RadiK called once per row (its batched API has one K for "
+                                         "all rows), built from its sources for sm_100a, on the GPU"}
+    else:
+        out["impl"] = "radik_b200"
+        out["gpu_launches"] = launches * args.steps
+        out["uneven"] = {"one_launch_ms": round(ms, 4), "per_row_ms": round(per_row_ms, 3),
+                         "per_row_gkeys": round(total_n / (per_row_ms / 1e3) / 1e9, 3),
+                         "speedup_vs_per_row": round(per_row_ms / ms, 2), "cuda_graph": True}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            import oracle
+
+            rows = min(B, 256)
+            t = time.perf_counter()
+            oracle.topk(x[:int(offs[rows - 1] + ns[rows - 1])], ns[:rows], ks[:rows], flags=oracle.flags_of(True, False),
+                        out_offsets=[int(v) for v in oo[:rows]])
+            dt = time.perf_counter() - t
+            keys = int(sum(ns[:rows]))
+            out["cpu_baseline"] = {"value": round(keys / dt / 1e9, 4), "unit": "Gkeys/s", "cores": oracle.max_threads(),
+                                   "kind": "port", "sample": f"the first {rows} rows ({keys} keys), OpenMP "
+                                                             f"nth_element per row"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_skew(args, dev, world, rank):
+    """Skew / adversarial sweep: single fp32 rows of n = 2^24, k = 2^4 .. 2^16,
+    four distributions (U(0,1); 1.0f with random low 8 mantissa bits; Zipf(1.1)
+    ranks; 90% one constant + 10% U(0,1)), largest-k, unsorted.  Each case is
+    timed per launch with L2 flushed between launches (a 64 MiB row fits L2).
+    value = geometric mean Gkeys/s over the cases; the table is in "sweep"."""
+    import torch
+
+    from radik_b200 import workloads
+
+    n = 1 << 24
+    ks = [1 << e for e in range(4, 17)]
+    dists = ["uniform", "mantissa_noise", "zipf", "constant_heavy"]
+    reps = max(3, min(args.steps, 10))
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    vals = torch.empty(max(ks), dtype=torch.float32, device=dev)
+    idx = torch.empty(max(ks), dtype=torch.int32, device=dev)
+    if args.impl == "reference":
+        import oracle
+
+        ref = oracle.RefRadik()
+        ws = torch.empty(ref.workspace_size(0, max(ks), n, 1), dtype=torch.uint8, device=dev)
+
+        def call(x, k):
+            ref.topk(0, True, False, False, False, x.data_ptr(), vals.data_ptr(), idx.data_ptr(), ws.data_ptr(), [n], k,
+                     stream.cuda_stream)
+    else:
+        import radik_b200 as rk
+
+        flags = rk.make_flags(True, False)
+        ws = torch.empty(rk.get_radix_select_l_workspace_size(rk.F32, max(ks), n, 1, flags), dtype=torch.uint8,
+                         device=dev)
+
+        def call(x, k):
+            rk.topk_radix_select_l(x, None, vals, idx, ws, [n], k, largest=True, ascend=False, need_sorting=False,
+                                   stream=stream)
+    sweep = []
+    clocks = None
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    for dname in dists:
+        x = torch.from_numpy(workloads.skew_row(dname, n, 11)).to(dev)
+        for k in ks:
+            for _ in range(args.warmup):
+                call(x, k)
+            ts = []
+            for _ in range(reps):
+                flush.zero_()
+                a, b = _events(1)[0]
+                a.record(stream)
+                call(x, k)
+                b.record(stream)
+                torch.cuda.synchronize(dev)
+                ts.append(a.elapsed_time(b))
+            ms = statistics.median(ts)
+            sweep.append({"dist": dname, "k": k, "ms": round(ms, 4), "gkeys": round(n / (ms / 1e3) / 1e9, 2)})
+        if args.impl != "reference":
+            rk.status(ws, stream)
+    clocks = sampler.stop()
+    g = float(np.exp(np.mean([np.log(c["gkeys"]) for c in sweep])))
+    total_ms = sum(c["ms"] for c in sweep)
+    peak, peak_kind = load_peaks()
+    ach = float(np.exp(np.mean([np.log((n * 4 + c["k"] * 8) / (c["ms"] / 1e3) / 1e9) for c in sweep])))
+    out = {"metric": "Gkeys/s & % HBM peak; uneven-batch speedup vs plain per-row; serving p50/p99",
+           "value": round(world * g, 3), "unit": "Gkeys/s", "n_gpus": world, "steps": reps, "warmup": args.warmup,
+           "ms_per_step": round(total_ms / len(sweep), 5), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic: four distributions from numpy Philox-4x32-10, seed 11",
+           "config": {"workload": "skew sweep, single fp32 rows n = 2^24, k = 2^4..2^16, U(0,1) / 1.0f + low-8-bit "
+                                  "mantissa noise / Zipf(1.1) ranks / 90% constant 0.5 + 10% U(0,1); largest, "
+                                  "unsorted; value = geometric mean over the 52 cases",
+                      "n": n, "l2": "L2 flushed (256 MiB write) before every timed launch",
+                      "parallelism": f"replicated per GPU x{world}"},
+           "e2e": {"value": round(world * g, 3), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                   "note": "device-resident inputs; the end-to-end copy cost is the batched workload's"},
+           "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
+                        "algorithmic_bytes_per_launch": "n*4 + k*8"},
+           "clocks": clocks, "sweep": sweep}
+    out["impl"] = "reference" if args.impl == "reference" else "radik_b200"
+    out["gpu_launches"] = None if args.impl == "reference" else len(sweep) * (args.warmup + reps)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="radik_b200", choices=["radik_b200", "reference"])
-    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS) + ["uneven", "skew"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="override the row count (profiling a smaller case)")
@@ -183,6 +461,18 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
+    if args.workload == "uneven":
+        run_uneven(args, dev, world, rank)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.workload == "skew":
+        run_skew(args, dev, world, rank)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     B, n, k, dts, sorted_, largest, desc = WORKLOADS[args.workload]
     if args.rows > 0:

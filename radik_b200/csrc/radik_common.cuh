@@ -112,7 +112,10 @@ struct alignas(16) RowState {
   int32_t src_len;     // entries in the phase-B source
   int32_t final_pass;  // phase B: the next filter is the last
   int32_t sb_count;    // phase B: entries compacted for the finisher
-  int32_t pad[15];
+  int32_t pad0;
+  uint64_t pb_min;     // phase B: least / greatest composite of the matched set
+  uint64_t pb_max;     //   seen by the current histogram pass
+  int32_t pad[10];
 };
 static_assert(sizeof(RowState) == 128, "RowState layout");
 

@@ -269,6 +269,9 @@ struct alignas(16) ItemDesc {
 };
 constexpr int kQ = 4;  // queue slots per team
 constexpr int kSideCandMax = 1 << 17;  // candidate sets the side team resolves itself (else phase B)
+// Batches of fewer rows leave the grid idle at their end, so there every set
+// too large for smem goes to phase B, which resolves it with all CTAs.
+constexpr int kSideResolveMinRows = 32;
 struct Ctrl {
   uint64_t full[kStages];   // ring slot filled
   uint64_t empty[kStages];  // ring slot drained by every consumer warp
@@ -1700,8 +1703,8 @@ struct Engine {
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kResolveHistOff);
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
     const int W = K::KB + rc.IB;
-    // entries in groups of four per thread, loaded before they are used
-    constexpr int U = 4;
+    // entries in groups of eight per thread, loaded before they are used
+    constexpr int U = 8;
     const int iters = (src_n + SideTeam::kSize * U - 1) / (SideTeam::kSize * U);
     auto for_entries = [&](auto&& fn) {
       for (int it = 0; it < iters; ++it) {
@@ -1809,7 +1812,7 @@ struct Engine {
                                 &p.hdr->status);
         smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
         post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
-      } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax)) {
+      } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax) && p.B >= kSideResolveMinRows) {
         side_cand_resolve(r, rc, c, 0, 0, rc.k, c);
       } else if (c >= rc.k && c <= rc.cand_cap) {
         to_phase_b(r, 1, c, 0, 0, rc.k, c);
@@ -1831,7 +1834,8 @@ struct Engine {
       post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
     } else if (mode == kModeCand) {
       const int src_n = min(m->st_candn, rc.cand_cap);
-      if (src_n <= kSideCandMax) side_cand_resolve(r, rc, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+      if (src_n <= kSideCandMax && p.B >= kSideResolveMinRows)
+        side_cand_resolve(r, rc, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
       else to_phase_b(r, 1, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeDefer) {
       to_phase_b(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
@@ -1845,20 +1849,28 @@ struct Engine {
     int32_t row[kPhaseBSlots];
     int32_t nch[kPhaseBSlots];
     int32_t c0[kPhaseBSlots + 1];
+    int32_t chunk;  // entries per work unit this pass
   };
 
   // Runs f(bits, pos, ok) over entries [a, b) of a phase-B source.
   template <typename Fn>
   __device__ void pb_source(const RowCtx& rc, int src, int64_t a, int64_t b, Fn&& fn) {
     if (src == 1) {
+      // candidate entries from L2, eight loads a thread in flight
+      constexpr int UE = 8;
       const uint64_t* cand = p.cand + rc.cand_off;
-      const int64_t cnt = b - a;
-      const int64_t iters = (cnt + FullTeam::kSize - 1) / FullTeam::kSize;
-      for (int64_t it = 0; it < iters; ++it) {
-        const int64_t i = a + it * FullTeam::kSize + FullTeam::tid();
-        const bool ok = i < b;
-        const uint64_t e = ok ? ld_cg_u64(cand + i) : 0ull;
-        fn((uint32_t)(e >> 32), (int64_t)(uint32_t)e, ok);
+      for (int64_t base = a; base < b; base += (int64_t)UE * FullTeam::kSize) {
+        uint64_t e[UE];
+#pragma unroll
+        for (int u = 0; u < UE; ++u) {
+          const int64_t i = base + (int64_t)u * FullTeam::kSize + FullTeam::tid();
+          e[u] = i < b ? ld_cg_u64(cand + i) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < UE; ++u) {
+          const int64_t i = base + (int64_t)u * FullTeam::kSize + FullTeam::tid();
+          fn((uint32_t)(e[u] >> 32), (int64_t)(uint32_t)e[u], i < b);
+        }
       }
     } else {
       for_range_v<FullTeam, ES, U>(p.val_in, rc.in_off, a, b, fn, [&](const uint4& x, int64_t pos0, bool ok) {
@@ -1873,6 +1885,16 @@ struct Engine {
   // filter).  Returns the number of chunks.
   __device__ int pb_table(PBTable* t, int nG, int want) {
     if (FullTeam::tid() == 0) {
+      // work units sized so the pass spreads over the whole grid (at least
+      // 2048 entries, at most kPhaseBChunk)
+      int64_t sum = 0;
+      for (int i = 0; i < nG; ++i) {
+        const RowState* rs = p.rs + p.large_list[i];
+        if (__ldcg(&rs->final_pass) == want) sum += __ldcg(&rs->src_len);
+      }
+      int64_t ch = (sum + gridDim.x - 1) / gridDim.x;
+      ch = (ch + 2047) / 2048 * 2048;
+      const int chunk = ch < 2048 ? 2048 : ch > kPhaseBChunk ? kPhaseBChunk : (int)ch;
       int c = 0;
       for (int i = 0; i < nG; ++i) {
         const int r = p.large_list[i];
@@ -1881,10 +1903,11 @@ struct Engine {
         const int len = __ldcg(&rs->src_len);
         t->row[i] = r;
         t->c0[i] = c;
-        t->nch[i] = (fp == want) ? (len + kPhaseBChunk - 1) / kPhaseBChunk : 0;
+        t->nch[i] = (fp == want) ? (len + chunk - 1) / chunk : 0;
         c += t->nch[i];
       }
       t->c0[nG] = c;
+      t->chunk = chunk;
     }
     FullTeam::sync();
     return t->c0[nG];
@@ -1906,6 +1929,8 @@ struct Engine {
           RowState* rs = p.rs + p.large_list[i];
           const int cnt = __ldcg(&rs->count), kr = __ldcg(&rs->krem);
           rs->final_pass = (cnt == kr || cnt <= kCapSB) ? 1 : 0;
+          rs->pb_min = ~0ull;
+          rs->pb_max = 0;
         }
       }
       grid_barrier<FullTeam>(p.hdr, p.spin_limit);
@@ -1929,12 +1954,26 @@ struct Engine {
         FullTeam::sync();
         const int sh = W - plen, sd = W - plen - D;
         const uint32_t dm = (uint32_t)NB - 1u;
-        const int64_t a = (int64_t)(w - t->c0[i]) * kPhaseBChunk, b = min((int64_t)len, a + kPhaseBChunk);
+        const int64_t a = (int64_t)(w - t->c0[i]) * t->chunk, b = min((int64_t)len, a + t->chunk);
+        uint64_t lo = ~0ull, hi = 0;
         pb_source(rc, src, a, b, [&](uint32_t bits, int64_t pos, bool ok) {
           const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
-          hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
+          const bool match = ok && shr64(c, sh) == prefix;
+          hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, match);
+          if (match) {
+            lo = min(lo, c);
+            hi = max(hi, c);
+          }
         });
-        FullTeam::sync();
+        // the matched set's extremes: a level that does not split the set
+        // lets the selection jump to their common prefix instead
+        uint64_t mn, mx;
+        block_minmax<FullTeam>(lo, hi, &mn, &mx, m);
+        RowState* rsw = p.rs + r;
+        if (FullTeam::tid() == 0 && mn != ~0ull) {
+          atomicMin(reinterpret_cast<unsigned long long*>(&rsw->pb_min), (unsigned long long)mn);
+          atomicMax(reinterpret_cast<unsigned long long*>(&rsw->pb_max), (unsigned long long)mx);
+        }
         uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
         for (int j = FullTeam::tid(); j < NB; j += FullTeam::kSize)
           if (hist[j]) atomicAdd(gh + j, hist[j]);
@@ -1964,8 +2003,16 @@ struct Engine {
             rs->count = krem;  // give up on this row: finish what is there
             rs->final_pass = 1;
           } else {
-            rs->prefix = (ld_cg_u64(&rs->prefix) << D) | bin;
-            rs->plen = plen + D;
+            const uint64_t mn = ld_cg_u64(&rs->pb_min), mx = ld_cg_u64(&rs->pb_max);
+            const int common = mn == mx ? W : __clzll((long long)(mn ^ mx)) - (64 - W);
+            if (mn != ~0ull && common > plen + D) {
+              // every matched entry fell in one bin: take all the bits they share
+              rs->prefix = shr64(mn, W - common);
+              rs->plen = common;
+            } else {
+              rs->prefix = (ld_cg_u64(&rs->prefix) << D) | bin;
+              rs->plen = plen + D;
+            }
             rs->krem = krem - (int)cum;
             rs->count = (int)cnt;
             rs->final_pass = ((int)cnt == krem - (int)cum || (int)cnt <= kCapSB) ? 1 : 0;
@@ -1997,7 +2044,7 @@ struct Engine {
         uint64_t* dst = p.pb_sb + (size_t)i * kCapSB;
         auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, kCapSB, &p.hdr->status); };
         auto flo = [&](const WarpBuf& s) { flush_out<VT>(p, s, octr, rc.out_off, rc.k); };
-        const int64_t a = (int64_t)(w - t->c0[i]) * kPhaseBChunk, b = min((int64_t)len, a + kPhaseBChunk);
+        const int64_t a = (int64_t)(w - t->c0[i]) * t->chunk, b = min((int64_t)len, a + t->chunk);
         pb_source(rc, src, a, b, [&](uint32_t bits, int64_t pos, bool ok) {
           const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
           const uint64_t tt = shr64(c, sh);

@@ -227,3 +227,42 @@ def test_status_is_clean_after_calls():
     ws = torch.empty(rk.get_radix_select_l_workspace_size(rk.F32, 256, n, 2), dtype=torch.uint8, device=DEV)
     rk.topk(t, 256, [n, n], workspace=ws, check=False)
     assert rk.status(ws) == 0
+
+
+def test_topk_rows_replayed_from_cuda_graph():
+    """The one-launch uneven form takes device descriptors and never blocks the
+    host, so it can be captured once and replayed on new data."""
+    ns, ks = workloads.uneven_rows(48, 21, 10, 20, 2048)
+    offs = np.concatenate([[0], np.cumsum(ns)[:-1]]).astype(np.int64)
+    oo = np.concatenate([[0], np.cumsum(ks)[:-1]]).astype(np.int64)
+    total_n, total_out = int(sum(ns)), int(sum(ks))
+    desc = np.zeros(len(ns), dtype=[("in_off", "<i8"), ("out_off", "<i8"), ("n", "<i4"), ("k", "<i4")])
+    desc["in_off"], desc["out_off"], desc["n"], desc["k"] = offs, oo, ns, ks
+    desc_dev = torch.from_numpy(desc.view(np.uint8).copy()).to(DEV)
+    flags = rk.make_flags(True, True)
+    ws = torch.empty(rk.get_rows_workspace_size(rk.F32, len(ns), total_n, max(ns), max(ks), flags),
+                     dtype=torch.uint8, device=DEV)
+    x = torch.empty(total_n, dtype=torch.float32, device=DEV)
+    vals = torch.empty(total_out, dtype=torch.float32, device=DEV)
+    idx = torch.empty(total_out, dtype=torch.int32, device=DEV)
+    L = rk.lib()
+
+    def call():
+        rk._check(L.radik_topk_rows(rk.F32, flags, x.data_ptr(), None, vals.data_ptr(), idx.data_ptr(), ws.data_ptr(),
+                                    ws.numel(), desc_dev.data_ptr(), len(ns), total_n, max(ns), max(ks),
+                                    torch.cuda.current_stream().cuda_stream))
+
+    x.copy_(torch.from_numpy(workloads.normal(total_n, 1)))
+    call()  # first call on the device outside the capture (sets up the launch configuration)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        call()
+    for seed in (2, 3):
+        host = workloads.normal(total_n, seed)
+        x.copy_(torch.from_numpy(host))
+        graph.replay()
+        torch.cuda.synchronize()
+        assert rk.status(ws) == 0
+        ov, oi = oracle.topk(host, ns, ks, flags=oracle.flags_of(True, True), out_offsets=[int(v) for v in oo])
+        assert_same_selection((vals.cpu().numpy(), idx.cpu().numpy()), (ov, oi), ns, ks, oo, True, f"seed {seed}")

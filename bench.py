@@ -430,13 +430,99 @@ def run_skew(args, dev, world, rank):
         print(json.dumps(out), flush=True)
 
 
+def run_serving(args, dev, world, rank):
+    """Serving loop: Poisson arrivals at 1k..50k requests/s; n in {32000,
+    128256, 2^20, 2^24} w.p. {0.4, 0.3, 0.2, 0.1}; k in {1, 50, 1024}; 25% fp16;
+    N(0,1) scores already on the device; 40 GiB budget.  The continuous-
+    batching server (radik_server, mode 0) against plain per-request launches
+    (mode 1) on the same trace.  Latency = submission to completion."""
+    import torch
+
+    import radik_b200 as rk
+    from radik_b200 import workloads
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; its per-request "
+                              "form is the mode-1 baseline reported in this workload's radik_b200 line"}))
+        return
+    rates = [1000, 5000, 10000, 20000, 50000]
+    R = 10000 if args.rows <= 0 else args.rows
+    g = workloads.rng(17)
+    classes = [32000, 128256, 1 << 20, 1 << 24]
+    pools = {}
+    for ci, n in enumerate(classes):
+        for half in (False, True):
+            bufs = []
+            for j in range(4):
+                x = workloads.normal(n, 100 * ci + 10 * j + int(half))
+                bufs.append(torch.from_numpy(x.astype(np.float16) if half else x).to(dev))
+            pools[(n, half)] = bufs
+    out_f32 = torch.empty(R * 1024, dtype=torch.float32, device=dev)
+    out_f16 = torch.empty(R * 1024, dtype=torch.float16, device=dev)
+    out_idx = torch.empty(R * 1024, dtype=torch.int32, device=dev)
+    ns = g.choice(classes, size=R, p=[0.4, 0.3, 0.2, 0.1])
+    ks = g.choice([1, 50, 1024], size=R)
+    halves = g.random(R) < 0.25
+    keys_total = int(ns.sum())
+    flags = rk.make_flags(True, False)
+    table = []
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    for rate in rates:
+        gaps = g.exponential(1e6 / rate, size=R)
+        arr = np.cumsum(gaps) - gaps[0]
+        items = []
+        for i in range(R):
+            n, k, half = int(ns[i]), int(ks[i]), bool(halves[i])
+            x = pools[(n, half)][i % 4]
+            vo = (out_f16 if half else out_f32)[i * 1024:]
+            items.append(rk.TraceItem(float(arr[i]), rk.F16 if half else rk.F32, flags, x.data_ptr(), n, k,
+                                      vo.data_ptr(), out_idx[i * 1024:].data_ptr()))
+        row = {"rate_rps": rate, "requests": R}
+        for mode, name in ((0, "batched"), (1, "per_request")):
+            with rk.Server(dev.index, mode=mode, max_n=1 << 24, max_k=1024, budget_bytes=40 << 30) as srv:
+                # warm-up: a few requests through the same server
+                srv.run_trace(items[:16])
+                t0 = time.perf_counter()
+                lat = np.asarray(srv.run_trace(items), dtype=np.float64)
+                wall = time.perf_counter() - t0
+            span_s = max(float(np.max(arr + lat)) / 1e6, 1e-9)
+            row[name] = {"p50_ms": round(float(np.percentile(lat, 50)) / 1e3, 4),
+                         "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 4),
+                         "throughput_rps": round(R / span_s, 1),
+                         "gkeys_per_s": round(keys_total / span_s / 1e9, 3), "wall_s": round(wall, 3)}
+        row["p99_speedup_vs_per_request"] = round(row["per_request"]["p99_ms"] / max(row["batched"]["p99_ms"], 1e-9), 2)
+        table.append(row)
+    clocks = sampler.stop()
+    top = table[-1]["batched"]
+    peak, peak_kind = load_peaks()
+    out = {"metric": "Gkeys/s & % HBM peak; uneven-batch speedup vs plain per-row; serving p50/p99",
+           "value": top["gkeys_per_s"], "unit": "Gkeys/s", "n_gpus": world, "steps": R, "warmup": 16,
+           "ms_per_step": top["p50_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32/f16", "data": "synthetic: N(0,1) score pools (numpy Philox), Poisson arrivals seed 17",
+           "config": {"workload": "serving: Poisson arrivals at 1k-50k req/s, n in {32000, 128256, 2^20, 2^24} "
+                                  "w.p. {.4,.3,.2,.1}, k in {1, 50, 1024}, 25% fp16, largest, unsorted, 40 GiB budget; "
+                                  "value = keys served per second at 50k req/s",
+                      "requests_per_rate": R, "l2": "score pools larger than L2 (64 MiB rows)",
+                      "parallelism": "one server per GPU"},
+           "e2e": {"value": top["gkeys_per_s"], "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                   "note": "requests' scores are produced on the device; latency is submission to completion"},
+           "roofline": {"bound": "hbm", "achieved": round(top["gkeys_per_s"] * 1e9 * 3.5 / 1e9, 1), "peak": peak,
+                        "unit": "GB/s", "frac": round(top["gkeys_per_s"] * 3.5 / peak, 4), "traffic": None,
+                        "peak_source": f"{peak_kind} hbm_gbs", "note": "offered load, not a bound: mean 3.5 B/key"},
+           "clocks": clocks, "serving": table, "impl": "radik_b200", "gpu_launches": None}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="radik_b200", choices=["radik_b200", "reference"])
-    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS) + ["uneven", "skew"])
+    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS) + ["uneven", "skew", "serving"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="override the row count (profiling a smaller case)")
@@ -467,8 +553,8 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    if args.workload == "skew":
-        run_skew(args, dev, world, rank)
+    if args.workload in ("skew", "serving"):
+        (run_skew if args.workload == "skew" else run_serving)(args, dev, world, rank)
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()

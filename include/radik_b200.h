@@ -97,6 +97,20 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
  * device_bits (nullable) receives the raw device status word. */
 int radik_get_status(void* workspace, void* stream, int* device_bits);
 
+/* Autotuner (no RadiK counterpart).  Times radik_topk on the caller's
+ * buffers with chunk lengths from a quarter to four times the built-in
+ * choice (4 runs each, CUDA events, the first discarded) and keeps the
+ * fastest for the call's shape bucket -- dtype, sortedness and log2 of the
+ * row count, longest row and K -- for every later radik_topk call in this
+ * process.  *chunk (nullable) receives the chosen length.  Synchronises the
+ * stream: do not call it inside a stream capture.  The outputs hold a valid
+ * result afterwards.  The environment variable RADIK_CH still overrides. */
+int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+                   void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream,
+                   int* chunk);
+/* Forgets every tuned shape. */
+void radik_autotune_reset(void);
+
 /* Size of the fixed device scratch behind radik_topk_static(). */
 #define RADIK_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
 
@@ -126,6 +140,63 @@ int radik_get_status(void* workspace, void* stream, int* device_bits);
  *     radik_get_status(*scratch, stream, ...) reads the call's device status. */
 int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
                       void* idx_out, const int* task_len, int task_num, int K, void* stream, void** scratch);
+
+/* ---- Serving: a continuous-batching request loop.  No RadiK counterpart:
+ * RadiK's callers form their own batches and call topKRadixSelectL once per
+ * batch.  A server owns a worker thread, batch slots (workspace, output
+ * staging, a stream each) and a device-memory budget.  Each request is one
+ * row already on the device; its results land in the request's own device
+ * buffers.  Requests that arrive while batches run are admitted into the next
+ * batch as a slot and budget allow, so several batches are in flight at once
+ * and their copies, planning and selection overlap on the device.  Each
+ * batch is one radik_topk_rows launch over the requests of one (dtype, flags)
+ * group; a request's result does not depend on the batch it joined (the
+ * selection is exact, ties go to the lowest positions). */
+typedef struct radik_server radik_server;
+
+typedef struct {
+  int device;              /* CUDA device the server works on */
+  int mode;                /* 0: continuous batching; 1: one radik_topk launch per request (baseline) */
+  int slots;               /* batches in flight at once (default 3; mode 1 uses 1) */
+  int max_batch_rows;      /* requests per batch (default 512) */
+  int64_t max_batch_keys;  /* sum of n per batch (default 2^27) */
+  int max_n;               /* largest request n (default 2^24) */
+  int max_k;               /* largest request k (default 2048) */
+  size_t budget_bytes;     /* device bytes of requests in flight (values + results; default 40 GiB) */
+} radik_server_config;
+
+typedef struct {
+  uint64_t id;        /* as returned by radik_server_submit */
+  int32_t status;     /* radik_status of the request's batch */
+  int32_t pad;
+  double latency_us;  /* submission to completion seen by the worker */
+} radik_completion;
+
+typedef struct {
+  double arrival_us;   /* offset from the start of the trace */
+  int dtype;
+  uint32_t flags;      /* RADIK_LARGEST / SORTED / ASCEND / IDX64 */
+  const void* values;  /* device, n values */
+  int n, k;
+  void* val_out;       /* device, k values */
+  void* idx_out;       /* device, k indices */
+} radik_trace_item;
+
+int radik_server_create(const radik_server_config* cfg, radik_server** server);
+/* Queues one request (thread-safe, returns at once).  WITHSCALE / WITHIDXIN
+ * requests are not served (RADIK_ENOTSUP). */
+int radik_server_submit(radik_server* server, int dtype, uint32_t flags, const void* values, int n, int k,
+                        void* val_out, void* idx_out, uint64_t* id);
+/* Moves up to max finished requests into out; *count receives how many. */
+int radik_server_poll(radik_server* server, radik_completion* out, int max, int* count);
+/* Blocks until every submitted request has finished; returns the first error. */
+int radik_server_drain(radik_server* server);
+/* Load generator: submits items at their arrival offsets from this host
+ * thread (busy-waiting between them), drains, and writes each item's latency
+ * (in item order) to latency_us.  No other thread may submit meanwhile. */
+int radik_server_run_trace(radik_server* server, const radik_trace_item* items, int count, double* latency_us);
+/* Finishes queued work, then frees the server. */
+int radik_server_destroy(radik_server* server);
 
 /* Human-readable text of a radik_status code. */
 const char* radik_strerror(int status);

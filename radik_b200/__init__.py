@@ -64,6 +64,11 @@ def lib() -> ctypes.CDLL:
     L.radik_topk.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp]
     L.radik_topk_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp]
     L.radik_get_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
+    L.radik_autotune.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
+                                 ctypes.POINTER(ctypes.c_int)]
+    L.radik_autotune.restype = ctypes.c_int
+    L.radik_autotune_reset.argtypes = []
+    L.radik_autotune_reset.restype = None
     L.radik_topk_static.argtypes = [i32, u32, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
                                     ctypes.POINTER(vp)]
     L.radik_strerror.argtypes = [i32]
@@ -277,3 +282,135 @@ def topk_static(values, k: int, lengths: Optional[Sequence[int]] = None, *, larg
         bits = ctypes.c_int(0)
         _check(lib().radik_get_status(scratch, _stream_handle(stream), ctypes.byref(bits)))
     return vals, idx
+
+
+# ---------------------------------------------------------------------------
+# Serving: continuous-batching request loop (radik_server_* in the C ABI)
+# ---------------------------------------------------------------------------
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("mode", ctypes.c_int), ("slots", ctypes.c_int),
+                ("max_batch_rows", ctypes.c_int), ("max_batch_keys", ctypes.c_int64), ("max_n", ctypes.c_int),
+                ("max_k", ctypes.c_int), ("budget_bytes", ctypes.c_size_t)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("latency_us", ctypes.c_double)]
+
+
+class TraceItem(ctypes.Structure):
+    _fields_ = [("arrival_us", ctypes.c_double), ("dtype", ctypes.c_int), ("flags", ctypes.c_uint32),
+                ("values", ctypes.c_void_p), ("n", ctypes.c_int), ("k", ctypes.c_int),
+                ("val_out", ctypes.c_void_p), ("idx_out", ctypes.c_void_p)]
+
+
+def _server_lib():
+    L = lib()
+    if not getattr(L, "_server_bound", False):
+        vp = ctypes.c_void_p
+        L.radik_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.radik_server_submit.argtypes = [vp, ctypes.c_int, ctypes.c_uint32, vp, ctypes.c_int, ctypes.c_int, vp, vp,
+                                          ctypes.POINTER(ctypes.c_uint64)]
+        L.radik_server_poll.argtypes = [vp, ctypes.POINTER(Completion), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.radik_server_drain.argtypes = [vp]
+        L.radik_server_run_trace.argtypes = [vp, ctypes.POINTER(TraceItem), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.radik_server_destroy.argtypes = [vp]
+        for name in ("radik_server_create", "radik_server_submit", "radik_server_poll", "radik_server_drain",
+                     "radik_server_run_trace", "radik_server_destroy"):
+            getattr(L, name).restype = ctypes.c_int
+        L._server_bound = True
+    return L
+
+
+class Server:
+    """Continuous-batching top-k server on one device (radik_server_*).
+
+    mode 0 batches queued requests into one-launch radik_topk_rows calls;
+    mode 1 is the per-request baseline (one radik_topk launch each).  Request
+    values and result buffers are device tensors owned by the caller and must
+    stay alive until the request completes.
+    """
+
+    def __init__(self, device: int = 0, mode: int = 0, slots: int = 0, max_batch_rows: int = 0,
+                 max_batch_keys: int = 0, max_n: int = 0, max_k: int = 0, budget_bytes: int = 0):
+        self._L = _server_lib()
+        cfg = ServerConfig(device, mode, slots, max_batch_rows, max_batch_keys, max_n, max_k, budget_bytes)
+        h = ctypes.c_void_p(0)
+        _check(self._L.radik_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, values, k: int, val_out, idx_out, *, largest: bool = True, sorted: bool = False,
+               ascend: Optional[bool] = None) -> int:
+        flags = make_flags(largest, sorted, ascend, False, False, idx_out.dtype.itemsize == 8)
+        rid = ctypes.c_uint64(0)
+        _check(self._L.radik_server_submit(self._h, dtype_code(values.dtype), flags, values.data_ptr(),
+                                           int(values.numel()), int(k), val_out.data_ptr(), idx_out.data_ptr(),
+                                           ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, max_items: int = 4096):
+        buf = (Completion * max_items)()
+        cnt = ctypes.c_int(0)
+        _check(self._L.radik_server_poll(self._h, buf, max_items, ctypes.byref(cnt)))
+        return [(buf[i].id, buf[i].status, buf[i].latency_us) for i in range(cnt.value)]
+
+    def drain(self) -> None:
+        _check(self._L.radik_server_drain(self._h))
+
+    def run_trace(self, items) -> "list":
+        """items: sequence of TraceItem; returns per-item latencies (us)."""
+        arr = (TraceItem * max(len(items), 1))(*items)
+        lat = (ctypes.c_double * max(len(items), 1))()
+        _check(self._L.radik_server_run_trace(self._h, arr, len(items), lat))
+        return list(lat)[:len(items)]
+
+    def close(self) -> None:
+        if self._h:
+            self._L.radik_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bool = True, sorted: bool = False,
+             workspace=None, stream=None) -> int:
+    """radik_autotune: times the chunk-length candidates on these buffers and
+    keeps the fastest for this shape bucket (dtype, sortedness, log2 of rows,
+    longest row, k) for later calls in this process.  Returns the chosen
+    chunk length.  Synchronises ``stream``."""
+    import torch
+
+    if values.dim() == 2:
+        B, n = values.shape
+        lengths = [n] * B
+        flat = values.contiguous().view(-1)
+    else:
+        lengths = list(lengths) if lengths is not None else [values.numel()]
+        flat = values.contiguous()
+        B = len(lengths)
+    flags = make_flags(largest, sorted)
+    dt = dtype_code(values.dtype)
+    if workspace is None:
+        workspace = torch.empty(get_radix_select_l_workspace_size(dt, k, max(lengths), B, flags), dtype=torch.uint8,
+                                device=values.device)
+    vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
+    idx = torch.empty((B, k), dtype=torch.int32, device=values.device)
+    arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
+    chunk = ctypes.c_int(0)
+    _check(lib().radik_autotune(dt, flags, flat.data_ptr(), None, vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(),
+                                workspace.numel(), arr, B, int(k), _stream_handle(stream), ctypes.byref(chunk)))
+    return chunk.value
+
+
+def autotune_reset() -> None:
+    lib().radik_autotune_reset()

@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libradik_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in (
-    "radik_engine_f32.cu", "radik_engine_f16.cu", "radik_engine_bf16.cu", "radik_plan.cu", "radik_api.cu")]
+    "radik_engine_f32.cu", "radik_engine_f16.cu", "radik_engine_bf16.cu", "radik_plan.cu", "radik_api.cu",
+    "radik_server.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("radik_common.cuh", "radik_engine.cuh")] + [
     os.path.join(ROOT, "include", "radik_b200.h")]
 OBJ_DIR = os.path.join(ROOT, "_build")
@@ -73,6 +74,26 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+CLI_SRC = os.path.join(HERE, "csrc", "radik_cli.cu")
+CLI_BIN = os.path.join(HERE, "bin", "test_radik_b200")
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> str:
+    """The RadiK-compatible benchmark driver (links libradik_b200.so)."""
+    deps = [CLI_SRC, LIB, os.path.join(ROOT, "include", "topk_radixselect.h")]
+    if not (force or _stale(CLI_BIN, deps)):
+        return CLI_BIN
+    os.makedirs(os.path.dirname(CLI_BIN), exist_ok=True)
+    cmd = [_nvcc(), "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-I" + os.path.join(ROOT, "include"),
+           "-o", CLI_BIN + ".tmp", CLI_SRC, "-L" + HERE, "-lradik_b200", "-lcurand", "-Xlinker", "-rpath",
+           "-Xlinker", "$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(CLI_BIN + ".tmp", CLI_BIN)
+    return CLI_BIN
+
+
 def build_oracle(verbose: bool = False) -> None:
     make = shutil.which("make")
     if make is None:
@@ -83,6 +104,7 @@ def build_oracle(verbose: bool = False) -> None:
 
 def build(force: bool = False, verbose: bool = False) -> None:
     build_library(force=force, verbose=verbose)
+    build_cli(force=force, verbose=verbose)
     build_oracle(verbose=verbose)
 
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -132,21 +133,51 @@ int env_int(const char* name, int dflt) {
 // Tunables: chunk lengths and first-digit width.  Single-read rows use
 // chunks of 4K..256K elements, aiming at about eight chunks per CTA so the
 // work queue balances (the last chunks bound the tail) while each chunk
-// streams long enough to amortise its item overhead.  Radix rows use 32K-element chunks: their filter items
-// re-read chunks that the histogram items read two grids earlier, and that
-// window (2 x 148 x 128 KB) must stay in L2.  The 14-bit first digit (16384
-// bins, 64 KB of smem) leaves about n/64 keys of an i.i.d. fp32 row in the
-// selected bin.  RADIK_CH / RADIK_CHR / RADIK_D1 override (tuning sweeps).
+// streams long enough to amortise its item overhead; radik_autotune can
+// replace that choice per shape bucket.  Radix rows use 32K-element chunks:
+// their filter items re-read chunks that the histogram items read two grids
+// earlier, and that window (2 x 148 x 128 KB) must stay in L2.  The 12-bit
+// first digit (4096 bins, 16 KB of smem) leaves about n/4096 keys of an
+// i.i.d. row in the selected bin.  RADIK_CH / RADIK_CHR / RADIK_D1 override
+// everything (tuning sweeps).
 struct Config {
   int CH, CHR, D1;
 };
 
-Config choose_config(int64_t stream_elems, int grid) {
+// Autotuned chunk lengths, per shape bucket (radik_autotune).
+std::mutex g_tune_mu;
+std::map<uint64_t, int> g_tuned_ch;
+
+int ilog2(int64_t v) {
+  int l = 0;
+  while (v > 1) {
+    v >>= 1;
+    ++l;
+  }
+  return l;
+}
+
+// Shape bucket of a call: dtype, form (uniform / rows), sorted, and the log2
+// of the row count, the longest row and k.
+uint64_t shape_bucket(int dtype, uint32_t flags, bool rows_form, int64_t B, int64_t n_max, int64_t K) {
+  return (uint64_t)dtype | ((uint64_t)rows_form << 2) | ((uint64_t)((flags & kFlagSorted) != 0) << 3) |
+         ((uint64_t)ilog2(std::max<int64_t>(B, 1)) << 4) | ((uint64_t)ilog2(std::max<int64_t>(n_max, 1)) << 12) |
+         ((uint64_t)ilog2(std::max<int64_t>(K, 1)) << 20);
+}
+
+int tuned_ch(uint64_t bucket) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  const auto it = g_tuned_ch.find(bucket);
+  return it == g_tuned_ch.end() ? 0 : it->second;
+}
+
+Config choose_config(int64_t stream_elems, int grid, uint64_t bucket) {
   Config c{};
   const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 8));
   int ch = kMinCH;
   while (ch < kMaxCH && ch * 2 <= target) ch *= 2;
-  c.CH = ch;
+  const int tc = tuned_ch(bucket);
+  c.CH = tc ? tc : ch;
   c.CHR = 32768;
   c.D1 = kMaxD1;
   const int ech = env_int("RADIK_CH", 0);
@@ -283,7 +314,9 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  const Config cfg = choose_config(multi_elems, grid);
+  int n_max_call = 0;
+  for (int i = 0; i < B; ++i) n_max_call = std::max(n_max_call, task_len[i]);
+  const Config cfg = choose_config(multi_elems, grid, shape_bucket(dtype, flags, false, B, n_max_call, K));
   // exact needs of this call
   int64_t na = 0, nb = 0, cand = 0, sortn = 0;
   bool has_radix = false;
@@ -371,7 +404,7 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  const Config cfg = choose_config(total_n, grid);
+  const Config cfg = choose_config(total_n, grid, shape_bucket(dtype, flags, true, B, n_max, k_max));
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, true), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -404,6 +437,67 @@ int radik_get_status(void* workspace, void* stream_, int* device_bits) {
   if (bits & kStatusTimeout) return fail(RADIK_ETIMEOUT, "radik: a device wait timed out");
   if (bits) return fail(RADIK_EINTERNAL, "radik: internal selection error");
   return RADIK_OK;
+}
+
+int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+                   void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream_,
+                   int* chunk) {
+  if (task_num <= 0 || K <= 0 || !task_len) return fail(RADIK_EINVAL, "radik_autotune: empty call");
+  int n_max = 0;
+  int64_t total = 0;
+  for (int i = 0; i < task_num; ++i) {
+    if (task_len[i] < 0) return fail(RADIK_EINVAL, "radik: negative task length");
+    n_max = std::max(n_max, task_len[i]);
+    total += task_len[i];
+  }
+  int grid = 0;
+  int rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
+  const uint64_t bucket = shape_bucket(dtype, flags, false, task_num, n_max, K);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return fail(RADIK_ECUDA, "cudaEventCreate");
+  // candidates: powers of two from a quarter to four times the default's pick
+  const Config dflt = choose_config(total, grid, ~0ull);
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int ch = std::max(kMinCH, dflt.CH / 4); ch <= std::min(kMaxCH, dflt.CH * 4); ch *= 2) {
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      g_tuned_ch[bucket] = ch;
+    }
+    float ms_sum = 0.f;
+    for (int rep = 0; rep < 4 && rc == RADIK_OK; ++rep) {
+      cudaEventRecord(a, stream);
+      rc = radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes, task_len, task_num,
+                      K, stream_);
+      cudaEventRecord(b, stream);
+      if (rc == RADIK_OK && cudaEventSynchronize(b) != cudaSuccess) rc = fail(RADIK_ECUDA, "cudaEventSynchronize");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) ms_sum += ms;  // the first run warms up
+    }
+    if (rc != RADIK_OK) break;
+    if (ms_sum < best_ms) {
+      best_ms = ms_sum;
+      best = ch;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (best) g_tuned_ch[bucket] = best;
+    else g_tuned_ch.erase(bucket);
+  }
+  if (rc != RADIK_OK) return rc;
+  if (chunk) *chunk = best;
+  return radik_get_status(workspace, stream_, nullptr);
+}
+
+void radik_autotune_reset(void) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned_ch.clear();
 }
 
 int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,

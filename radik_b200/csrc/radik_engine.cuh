@@ -218,7 +218,7 @@ constexpr int kHistOff = 0;                             // first-digit histogram
 constexpr int kResolveHistOff = kCapSB * 8;             // 4096-bin histogram behind a finisher's entries
 constexpr int kSmemRowHistOff = kSmemRowCap * 4;        // behind an smem row's values
 constexpr int kSampleHistOff = kSampleMax * 4;          // behind the sampled keys
-constexpr int kSampleRawOff = kSampleHistOff + 16384;   // 16-bit sampled values before conversion
+constexpr int kSampleRawOff = kSampleHistOff + 1024;    // 16-bit sampled values before conversion
 static_assert(24 * kSinkPf * 8 <= kConsAreaBytes, "pre-filter staging");
 static_assert(24 * (kSinkCand + kSinkOut) * 8 <= kConsAreaBytes, "filter staging");
 static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B staging");
@@ -226,7 +226,7 @@ static_assert((4 << kMaxD1) <= kConsAreaBytes, "histogram");
 static_assert(kResolveHistOff + 16384 <= kSideAreaBytes, "finisher area");
 static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
 static_assert(32 * 128 * 8 <= kSideAreaBytes, "phase-B staging");
-static_assert(kSampleHistOff + 16384 <= kSideAreaBytes, "sample area");
+static_assert(kSampleHistOff + 1024 <= kSideAreaBytes, "sample area");
 static_assert(kSampleRawOff + kSampleMax * 2 <= kSideAreaBytes, "16-bit sample staging");
 
 struct Misc {

@@ -84,3 +84,9 @@ def test_flag_helper():
     f = rk.make_flags(largest=True, sorted=True)
     assert f == rk.LARGEST | rk.SORTED
     assert rk.make_flags(largest=False) == rk.ASCEND
+
+
+def test_autotune_rejects_empty_call_without_device():
+    arr = (ctypes.c_int * 1)(0)
+    rc = rk.lib().radik_autotune(rk.F32, 0, 1 << 12, None, 1 << 12, 1 << 12, 1 << 12, 1 << 20, arr, 0, 4, None, None)
+    assert rc == rk.EINVAL

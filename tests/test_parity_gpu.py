@@ -266,3 +266,17 @@ def test_topk_rows_replayed_from_cuda_graph():
         assert rk.status(ws) == 0
         ov, oi = oracle.topk(host, ns, ks, flags=oracle.flags_of(True, True), out_offsets=[int(v) for v in oo])
         assert_same_selection((vals.cpu().numpy(), idx.cpu().numpy()), (ov, oi), ns, ks, oo, True, f"seed {seed}")
+
+
+def test_autotune_keeps_results_exact():
+    n, B, k = 1 << 20, 32, 256
+    flat = np.concatenate([values_for(rk.F32, n, "normal", 900 + r) for r in range(B)])
+    t = to_dev(flat, rk.F32).view(B, n)
+    before = rk.topk(t, k, largest=True, sorted=True)
+    try:
+        ch = rk.autotune(t, k, largest=True, sorted=True)
+        assert ch >= 4096 and (ch & (ch - 1)) == 0
+        after = rk.topk(t, k, largest=True, sorted=True)
+        assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])
+    finally:
+        rk.autotune_reset()

@@ -278,6 +278,7 @@ struct Ctrl {
   uint64_t cq_full[kQ], cq_empty[kQ], sq_full[kQ], sq_empty[kQ];
   ItemDesc cq[kQ], sq[kQ];
   uint32_t side_done;       // side items finished (written by the side team)
+  uint32_t cons_done;       // consumer items finished (written by the consumer team)
   int32_t first_q;          // the CTA's first claim
 };
 static_assert(kCtrlOff + 2 * 3072 + sizeof(Ctrl) <= kSmemBytes, "control area");
@@ -1377,8 +1378,9 @@ struct Engine {
   }
 
   // ---- FIN item: wait for the row's chunk items, then finish the row
-  __device__ void fin_item(int r, const RowCtx& rc) {
-    if (SideTeam::tid() == 0) {
+  template <class Tm>
+  __device__ void fin_item_t(int r, const RowCtx& rc) {
+    if (Tm::tid() == 0) {
       const int32_t* t = &p.rs[r].fticket;
       uint32_t it = 0;
       while (ld_acquire(t) < rc.fin_wait) {
@@ -1389,9 +1391,10 @@ struct Engine {
         __nanosleep(128);
       }
     }
-    SideTeam::sync();
-    finish_row(r);
-  }
+    Tm::sync();
+    finish_row<Tm>(r);
+  }  __device__ void fin_item(int r, const RowCtx& rc) { fin_item_t<SideTeam>(r, rc); }
+
 
   // ---- sample item of a pre-filter row: publish the threshold
   template <class Tm>
@@ -1674,8 +1677,9 @@ struct Engine {
   }
 
   // Hands a row to phase B.
+  template <class Tm>
   __device__ void to_phase_b(int r, int src, int src_len, uint64_t prefix, int plen, int krem, int count) {
-    if (SideTeam::tid() == 0) {
+    if (Tm::tid() == 0) {
       RowState* rs = p.rs + r;
       rs->src = src;
       rs->src_len = src_len;
@@ -1696,6 +1700,7 @@ struct Engine {
   // smem: 12-bit histogram levels over the region (read from L2) until the
   // matched set fits in smem or equals krem, then one pass that emits the
   // better entries and gathers the matched ones into smem to resolve there.
+  template <class Tm>
   __device__ void side_cand_resolve(int r, const RowCtx& rc, int src_n, uint64_t prefix, int plen, int krem,
                                     int count) {
     RowState* rs = p.rs + r;
@@ -1705,18 +1710,18 @@ struct Engine {
     const int W = K::KB + rc.IB;
     // entries in groups of eight per thread, loaded before they are used
     constexpr int U = 8;
-    const int iters = (src_n + SideTeam::kSize * U - 1) / (SideTeam::kSize * U);
+    const int iters = (src_n + Tm::kSize * U - 1) / (Tm::kSize * U);
     auto for_entries = [&](auto&& fn) {
       for (int it = 0; it < iters; ++it) {
         uint64_t e[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int i = (it * U + u) * SideTeam::kSize + SideTeam::tid();
+          const int i = (it * U + u) * Tm::kSize + Tm::tid();
           e[u] = i < src_n ? ld_cg_u64(cand + i) : 0ull;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int i = (it * U + u) * SideTeam::kSize + SideTeam::tid();
+          const int i = (it * U + u) * Tm::kSize + Tm::tid();
           const uint32_t bits = (uint32_t)(e[u] >> 32);
           const int64_t pos = (int64_t)(uint32_t)e[u];
           const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
@@ -1727,34 +1732,34 @@ struct Engine {
     for (int guard = 0; guard < 8 && count != krem && count > kCapSB && plen < W; ++guard) {
       const int D = min(12, W - plen);
       const int NB = 1 << D;
-      for (int i = SideTeam::tid(); i < NB; i += SideTeam::kSize) hist[i] = 0;
-      SideTeam::sync();
+      for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+      Tm::sync();
       const int sh = W - plen, sd = W - plen - D;
       const uint32_t dm = (uint32_t)NB - 1u;
       for_entries([&](uint32_t, int64_t, uint64_t c, bool ok) {
         hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
       });
-      SideTeam::sync();
-      block_select<SideTeam, false>(hist, NB, (uint32_t)krem, m);
+      Tm::sync();
+      block_select<Tm, false>(hist, NB, (uint32_t)krem, m);
       if (!m->sel_found) {
-        if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
+        if (Tm::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
         return;
       }
       prefix = (prefix << D) | m->sel_bin;
       plen += D;
       krem -= (int)m->sel_cum;
       count = (int)m->sel_cnt;
-      SideTeam::sync();
+      Tm::sync();
     }
     if (count != krem && count > kCapSB) {
-      if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusLevels);
+      if (Tm::tid() == 0) atomicOr(&p.hdr->status, kStatusLevels);
       return;
     }
     const bool final_mode = count == krem;
     const int sh = W - plen;
     uint32_t* out_ctr = reinterpret_cast<uint32_t*>(&rs->out_count);
-    if (SideTeam::tid() == 0) m->counter = 0;
-    SideTeam::sync();
+    if (Tm::tid() == 0) m->counter = 0;
+    Tm::sync();
     for_entries([&](uint32_t bits, int64_t pos, uint64_t c, bool ok) {
       const uint64_t t = shr64(c, sh);
       const bool to_out = ok && (t < prefix || (final_mode && t == prefix));
@@ -1765,7 +1770,7 @@ struct Engine {
       const uint32_t se = warp_reserve(to_ent ? 1u : 0u, &m->counter);
       if (to_ent && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
     });
-    SideTeam::sync();
+    Tm::sync();
     if (!final_mode) {
       const int ne = min((int)m->counter, kCapSB);
       auto get = [&](int i, uint32_t& bits, int64_t& pos) {
@@ -1773,19 +1778,20 @@ struct Engine {
         bits = (uint32_t)(e >> 32);
         pos = (int64_t)(uint32_t)e;
       };
-      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne,
+      smem_resolve<Tm, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne,
                                         reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m, &p.hdr->status);
-      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      smem_emit<Tm, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
     }
-    post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+    post_process<Tm, VT, SCALE>(p, rc, smem, m);
   }
 
   // Finisher work of a large row (all of its items are done).
+  template <class Tm>
   __device__ void finish_row(int r) {
     const RowCtx rc = load_row<VT, SCALE>(p, r);
     RowState* rs = p.rs + r;
     __threadfence();
-    if (SideTeam::tid() == 0) {
+    if (Tm::tid() == 0) {
       m->st_mode = rc.kind == kKindAll ? kModeAll : __ldcg(&rs->mode);
       m->st_krem = __ldcg(&rs->krem);
       m->st_count = __ldcg(&rs->count);
@@ -1793,7 +1799,7 @@ struct Engine {
       m->st_prefix = ld_cg_u64(&rs->prefix);
       m->st_candn = __ldcg(&rs->cand_count);
     }
-    SideTeam::sync();
+    Tm::sync();
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
     auto get = [&](int i, uint32_t& bits, int64_t& pos) {
       const uint64_t e = ent[i];
@@ -1804,43 +1810,43 @@ struct Engine {
     if (rc.kind == kKindGridPref) {
       const int c = m->st_candn;
       if (c >= rc.k && c <= kCapSB) {
-        load_entries<SideTeam>(ent, cand, c);
-        SideTeam::sync();
+        load_entries<Tm>(ent, cand, c);
+        Tm::sync();
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<SideTeam, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+        smem_resolve<Tm, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                                 &p.hdr->status);
-        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
-        post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+        smem_emit<Tm, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        post_process<Tm, VT, SCALE>(p, rc, smem, m);
       } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax) && p.B >= kSideResolveMinRows) {
-        side_cand_resolve(r, rc, c, 0, 0, rc.k, c);
+        side_cand_resolve<Tm>(r, rc, c, 0, 0, rc.k, c);
       } else if (c >= rc.k && c <= rc.cand_cap) {
-        to_phase_b(r, 1, c, 0, 0, rc.k, c);
+        to_phase_b<Tm>(r, 1, c, 0, 0, rc.k, c);
       } else {
-        to_phase_b(r, 0, rc.n, 0, 0, rc.k, rc.n);
+        to_phase_b<Tm>(r, 0, rc.n, 0, 0, rc.k, rc.n);
       }
       return;
     }
     const int mode = m->st_mode;
     if (mode == kModeSB) {
       const int ne = min(m->st_candn, kCapSB);
-      load_entries<SideTeam>(ent, cand, ne);
+      load_entries<Tm>(ent, cand, ne);
       uint64_t prefix = m->st_prefix;
       int plen = m->st_plen, krem = m->st_krem;
-      SideTeam::sync();
-      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+      Tm::sync();
+      smem_resolve<Tm, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                               &p.hdr->status);
-      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
-      post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+      smem_emit<Tm, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      post_process<Tm, VT, SCALE>(p, rc, smem, m);
     } else if (mode == kModeCand) {
       const int src_n = min(m->st_candn, rc.cand_cap);
       if (src_n <= kSideCandMax && p.B >= kSideResolveMinRows)
-        side_cand_resolve(r, rc, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
-      else to_phase_b(r, 1, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+        side_cand_resolve<Tm>(r, rc, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+      else to_phase_b<Tm>(r, 1, src_n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeDefer) {
-      to_phase_b(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
+      to_phase_b<Tm>(r, 0, rc.n, m->st_prefix, m->st_plen, m->st_krem, m->st_count);
     } else if (mode == kModeFinal || mode == kModeAll) {
-      post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+      post_process<Tm, VT, SCALE>(p, rc, smem, m);
     }
   }
 
@@ -2187,7 +2193,8 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
   auto throttle = [&](int last_q) {
     if (fin_tail > 0 && last_q + 1 >= NQ - fin_tail) {
       uint32_t it = 0;
-      while (*reinterpret_cast<volatile uint32_t*>(&ctl->side_done) < si) {
+      while (*reinterpret_cast<volatile uint32_t*>(&ctl->side_done) < si ||
+             *reinterpret_cast<volatile uint32_t*>(&ctl->cons_done) < ci) {
         if (++it > p.spin_limit) {
           atomicOr(&p.hdr->status, kStatusTimeout);
           break;
@@ -2213,7 +2220,10 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     d.fin = ir.fin;
     d.sub = ir.isA ? ir.sub - rc.a0 : (p.uniform ? ir.sub : ir.sub - rc.b0);
     if (!is_streaming(rc.kind, ir.isA, ir.fin)) {
-      push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
+      // Finishes in the tail of the claim order go to the consumer team (three
+      // times the side team's threads): nothing streams after them.
+      if (ir.fin && fin_tail > 0 && q >= NQ - fin_tail) push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
+      else push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
       throttle(q);
       q = (int)atomicAdd(&p.hdr->qhead, 1u);
       continue;
@@ -2320,6 +2330,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     }
     mbar_fence_init();
     ctl->side_done = 0;
+    ctl->cons_done = 0;
     for (Misc* mm : {cons_misc(smem), side_misc(smem)}) {
       mm->rel_row = -1;
       mm->t_row = -1;
@@ -2379,7 +2390,15 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
       if (ConsTeam::tid() == 0) m->rel_row = -1;
       if (d.q < 0) break;
       const RowCtx rc = load_row<VT, SCALE>(p, d.row);
-      if (d.isA) {
+      if (d.fin) {
+        // A finish from the tail of the claim order: this team has streamed
+        // all of its chunks and no copies follow, so the ring is its scratch.
+        // Its own last chunk may belong to this row: release it first.
+        e.do_release();
+        ConsTeam::sync();
+        Engine<VT, SCALE> ef(p, smem, smem, m);
+        ef.template fin_item_t<ConsTeam>(d.row, rc);
+      } else if (d.isA) {
         if (rc.kind == kKindAll) e.all_item(d.row, rc, d);
         else e.h_item(d.row, rc, d);
       } else if (rc.kind == kKindGridPref) {
@@ -2388,6 +2407,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
         e.f_item(d.row, rc, d);
       }
       ConsTeam::sync();
+      if (ConsTeam::tid() == 0) *reinterpret_cast<volatile uint32_t*>(&ctl->cons_done) = i + 1;
     }
     e.do_release();
   } else {

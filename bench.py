@@ -7,7 +7,13 @@ is one radik_topk call over the whole batch.  The inputs (1 GiB) are larger
 than L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl radik_b200|reference]
-                  [--workload batched|batched_k32|batched_k1024|batched_f16|single|skew|uneven]
+                  [--workload batched|batched_k32|batched_k1024|batched_f16|batched_sorted|single
+                              |uneven|skew|serving]
+
+uneven: 4096 rows of log-uniform n and per-row k, one radik_topk_rows launch
+replayed from a CUDA graph, beside the plain per-row form.  skew: single
+2^24 rows, k = 2^4..2^16, four distributions.  serving: Poisson arrivals
+through the continuous-batching server and through per-request launches.
 
 --impl reference runs the reference RadiK (topKRadixSelectL compiled from the
 reference's own sources into oracle/_ref/libradik_ref.so) on the same

@@ -36,10 +36,10 @@ enum : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 constexpr int kThreads = 1024;           // one CTA per SM: 24 consumer, 7 side, 1 producer warp
 constexpr int kCtasPerSM = 1;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCapSB = 7168;             // candidates a finisher resolves in smem (56 KB)
+constexpr int kCapSB = 6144;             // candidates a finisher resolves in smem (48 KB)
 constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
 constexpr int kCtaRowCap = 1 << 18;      // rows this short are selected by one CTA
-constexpr int kCapSort = 8192;           // outputs a finisher sorts in smem (64 KB)
+constexpr int kCapSort = 4096;           // outputs a finisher sorts in smem (32 KB)
 constexpr int kMaxD1 = 12;               // widest first digit (16 KB smem hist)
 constexpr int kMinD1 = 8;
 constexpr int kPrefRatio = 64;           // pre-filter rows with k * 64 <= n
@@ -47,7 +47,7 @@ constexpr int kSampleMax = 8192;         // sampled keys per row (32 KB smem)
 constexpr int kSampleMin = 1024;
 constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
 constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)
-constexpr int kSmemBytes = 224 * 1024;   // dynamic smem per CTA
+constexpr int kSmemBytes = 226 * 1024;   // dynamic smem per CTA
 constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scratch
 
 // Row kinds (a function of n and k only).

@@ -201,21 +201,21 @@ __device__ __forceinline__ uint32_t out_key_inv(uint32_t k, bool ascend) {
 //   consumer area  per-warp staging buffers / first-digit histogram
 //   side area      sampled keys, candidate entries, sort and resolve scratch
 //   control        per-team scratch (Misc), ring and queue mbarriers
-constexpr int kStages = 5;
+constexpr int kStages = 6;
 constexpr int kStageVecs = 24 * 32 * 2;                 // two 16-byte vectors per consumer thread
 constexpr int kStageBytes = kStageVecs * 16;            // 24 KB
-constexpr int kRingBytes = kStages * kStageBytes;       // 120 KB
+constexpr int kRingBytes = kStages * kStageBytes;       // 144 KB
 constexpr int kConsAreaOff = kRingBytes;
 constexpr int kConsAreaBytes = 24 * 1024;
 constexpr int kSideAreaOff = kConsAreaOff + kConsAreaBytes;
-constexpr int kSideAreaBytes = 72 * 1024;
-constexpr int kCtrlOff = kSideAreaOff + kSideAreaBytes;  // 216 KB
+constexpr int kSideAreaBytes = 50 * 1024;
+constexpr int kCtrlOff = kSideAreaOff + kSideAreaBytes;  // 218 KB
 constexpr int kSinkCand = 96;                           // filter items: candidate entries per warp
 constexpr int kSinkOut = 32;                            // filter / copy items: output entries per warp
 constexpr int kSinkPf = 128;                            // pre-filter items: candidate entries per warp
 // offsets inside an area
 constexpr int kHistOff = 0;                             // first-digit histogram (<= 16 KB)
-constexpr int kResolveHistOff = kCapSB * 8;             // 4096-bin histogram behind a finisher's entries
+constexpr int kResolveHistOff = kCapSB * 8;             // 256-bin histogram behind a finisher's entries
 constexpr int kSmemRowHistOff = kSmemRowCap * 4;        // behind an smem row's values
 constexpr int kSampleHistOff = kSampleMax * 4;          // behind the sampled keys
 constexpr int kSampleRawOff = kSampleHistOff + 1024;    // 16-bit sampled values before conversion
@@ -223,7 +223,7 @@ static_assert(24 * kSinkPf * 8 <= kConsAreaBytes, "pre-filter staging");
 static_assert(24 * (kSinkCand + kSinkOut) * 8 <= kConsAreaBytes, "filter staging");
 static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert((4 << kMaxD1) <= kConsAreaBytes, "histogram");
-static_assert(kResolveHistOff + 16384 <= kSideAreaBytes, "finisher area");
+static_assert(kResolveHistOff + 1024 <= kSideAreaBytes && 16384 <= kSideAreaBytes, "finisher area");
 static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
 static_assert(32 * 128 * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert(kSampleHistOff + 1024 <= kSideAreaBytes, "sample area");
@@ -1705,7 +1705,7 @@ struct Engine {
                                     int count) {
     RowState* rs = p.rs + r;
     const uint64_t* cand = p.cand + rc.cand_off;
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kResolveHistOff);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem);  // 12-bit levels; ent[] reuses it after the last
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
     const int W = K::KB + rc.IB;
     // entries in groups of eight per thread, loaded before they are used

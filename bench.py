@@ -51,8 +51,8 @@ WORKLOADS = {
 # workloads whose capture is summarised under profiles/ (the 256-row figure is
 # the 64-row capture scaled by rows: traffic grows with the rows streamed).
 NCU_TRAFFIC = {
-    ("batched", 256): 4 * (274446592 + 5250048),  # profiles/engine_kernel_f32_64x1M_k256_full.md
-    ("batched", 64): 274446592 + 5250048,
+    ("batched", 256): 4 * (270063360 + 4457728),  # profiles/engine_kernel_f32_64x1M_k256_full.md
+    ("batched", 64): 270063360 + 4457728,
 }
 
 

@@ -176,6 +176,10 @@ Config choose_config(int64_t stream_elems, int grid, uint64_t bucket) {
   const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 8));
   int ch = kMinCH;
   while (ch < kMaxCH && ch * 2 <= target) ch *= 2;
+  // Few large rows (2^24 keys or more in all): per-item overhead outweighs
+  // balance, so no chunk is shorter than 128K keys (single 2^24-key rows:
+  // 154 -> 111 us from 8K to 128K chunks).
+  if (stream_elems >= ((int64_t)1 << 24)) ch = std::max(ch, 1 << 17);
   const int tc = tuned_ch(bucket);
   c.CH = tc ? tc : ch;
   c.CHR = 32768;

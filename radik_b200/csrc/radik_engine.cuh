@@ -1010,24 +1010,21 @@ __device__ void post_process(const EngineParams& p, const RowCtx& rc, uint8_t* s
 // ----------------------------------------------------------------------------
 template <class Tm>
 __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
+  // bar_count only grows during a call (the header is cleared per call):
+  // every CTA takes the barriers in the same order, so barrier b completes at
+  // (b + 1) * gridDim.x arrivals -- one atomic per CTA, then a poll.
   Tm::sync();
   if (Tm::tid() == 0) {
-    const uint32_t gen = ld_acquire(&h->bar_gen);
     __threadfence();
-    const uint32_t arrived = atomicAdd(&h->bar_count, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(&h->bar_count, 0u);
-      __threadfence();
-      st_release(&h->bar_gen, gen + 1u);
-    } else {
-      uint32_t it = 0;
-      while (ld_acquire(&h->bar_gen) == gen) {
-        if (++it > spin_limit) {
-          atomicOr(&h->status, kStatusTimeout);
-          break;
-        }
-        __nanosleep(64);
+    const uint32_t old = atomicAdd(&h->bar_count, 1u);
+    const uint32_t target = (old / gridDim.x + 1u) * gridDim.x;
+    uint32_t it = 0;
+    while (ld_acquire(&h->bar_count) < target) {
+      if (++it > spin_limit) {
+        atomicOr(&h->status, kStatusTimeout);
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
   }
@@ -1689,6 +1686,8 @@ struct Engine {
       rs->count = count;
       rs->final_pass = 0;
       rs->sb_count = 0;
+      rs->pb_min = ~0ull;
+      rs->pb_max = 0;
       __threadfence();
       const int slot = atomicAdd(&p.hdr->nlarge, 1);
       p.large_list[slot] = r;
@@ -1926,12 +1925,14 @@ struct Engine {
       const int nL = __ldcg(&p.hdr->nlarge);
       if (nL <= 0) return;
       const int nG = min(nL, kPhaseBSlots);
-      // rows already small enough skip the histogram; each row's histogram
-      // slot is cleared here (the call clears the ring only for radix rows)
-      for (int i = blockIdx.x; i < nG; i += gridDim.x) {
+      // Round 0: every histogram slot is cleared (the call clears the ring only
+      // for radix rows; later each selection clears the slot it read), and
+      // rows already small enough skip the histogram.  Rows reaching the
+      // window later start from to_phase_b's state.
+      for (int i = blockIdx.x; round == 0 && i < kPhaseBSlots; i += gridDim.x) {
         uint32_t* gh = p.hist_ring + (size_t)i * ((size_t)1 << kMaxD1);
         for (int j = FullTeam::tid(); j < 4096; j += FullTeam::kSize) gh[j] = 0;
-        if (FullTeam::tid() == 0) {
+        if (FullTeam::tid() == 0 && i < nG) {
           RowState* rs = p.rs + p.large_list[i];
           const int cnt = __ldcg(&rs->count), kr = __ldcg(&rs->krem);
           rs->final_pass = (cnt == kr || cnt <= kCapSB) ? 1 : 0;
@@ -1939,7 +1940,7 @@ struct Engine {
           rs->pb_max = 0;
         }
       }
-      grid_barrier<FullTeam>(p.hdr, p.spin_limit);
+      if (round == 0) grid_barrier<FullTeam>(p.hdr, p.spin_limit);
       // ---- histogram of the next 12-bit digit
       int total = pb_table(t, nG, 0);
       uint32_t* hist = reinterpret_cast<uint32_t*>(smem);
@@ -2010,6 +2011,8 @@ struct Engine {
             rs->final_pass = 1;
           } else {
             const uint64_t mn = ld_cg_u64(&rs->pb_min), mx = ld_cg_u64(&rs->pb_max);
+            rs->pb_min = ~0ull;  // for the next round's histogram pass
+            rs->pb_max = 0;
             const int common = mn == mx ? W : __clzll((long long)(mn ^ mx)) - (64 - W);
             if (mn != ~0ull && common > plen + D) {
               // every matched entry fell in one bin: take all the bits they share

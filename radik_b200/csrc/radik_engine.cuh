@@ -1067,8 +1067,9 @@ struct Engine {
   __device__ void do_release() {
     if (pending_rel >= 0) {
       if (ConsTeam::tid() == ConsTeam::kSize - 32) {
-        __threadfence();
-        atomicAdd(&p.rs[pending_rel].fticket, 1);
+        // one release reduction: orders every consumer's candidate writes
+        // (seen through the team barrier) before the count the FIN acquires
+        asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.rs[pending_rel].fticket) : "memory");
       }
       pending_rel = -1;
     }

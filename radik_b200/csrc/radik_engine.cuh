@@ -205,6 +205,12 @@ constexpr int kStages = 6;
 constexpr int kStageVecs = 24 * 32 * 2;                 // two 16-byte vectors per consumer thread
 constexpr int kStageBytes = kStageVecs * 16;            // 24 KB
 constexpr int kRingBytes = kStages * kStageBytes;       // 144 KB
+// Stages a dtype's engine cycles through.  16-bit rows carry twice the keys
+// per stage, so their consumers hold a stage longer; there the sixth stage
+// cost more than it gave (fp16 256 x 2^20, k = 256: 1404 vs 1378 Gkeys/s with
+// five), while fp32 gains from it (1242 vs 1218).
+template <int VT>
+__host__ __device__ constexpr int ring_stages() { return VT == kF32 ? kStages : kStages - 1; }
 constexpr int kConsAreaOff = kRingBytes;
 constexpr int kConsAreaBytes = 24 * 1024;
 constexpr int kSideAreaOff = kConsAreaOff + kConsAreaBytes;
@@ -1104,7 +1110,8 @@ struct Engine {
     // checks; the slot and its phase parity advance without divisions.
     constexpr int kPer = kStageVecs / ConsTeam::kSize;
     const uint4* ring = reinterpret_cast<const uint4*>(base) + ConsTeam::tid();
-    uint32_t slot = d.g0 % kStages, parity = (d.g0 / kStages) & 1u;
+    constexpr uint32_t NS = ring_stages<VT>();
+    uint32_t slot = d.g0 % NS, parity = (d.g0 / NS) & 1u;
     const int nfull = (int)(d.nvec / kStageVecs);
     int64_t pos = d.va + (int64_t)ConsTeam::tid() * VEC;  // first element of this thread's vector in the stage
     for (int i = 0; i < d.nst; ++i) {
@@ -1131,7 +1138,7 @@ struct Engine {
       pos += (int64_t)kStageVecs * VEC;
       __syncwarp();
       if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
-      if (++slot == (uint32_t)kStages) {
+      if (++slot == NS) {
         slot = 0;
         parity ^= 1u;
       }
@@ -2273,9 +2280,10 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
     uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
     for (int i = 0; i < d.nst; ++i, ++g) {
-      const uint32_t slot = g % kStages;
-      if (g >= (uint32_t)kStages) {
-        const uint32_t parity = ((g / kStages) - 1u) & 1u;
+      constexpr uint32_t NS = ring_stages<VT>();
+      const uint32_t slot = g % NS;
+      if (g >= NS) {
+        const uint32_t parity = ((g / NS) - 1u) & 1u;
         uint32_t it = 0;
         while (!mbar_try_wait(&ctl->empty[slot], parity)) {
           if (++it > p.spin_limit) {
@@ -2322,7 +2330,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   Ctrl* ctl = ctrl_of(smem);
   if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kStages; ++i) {
+    for (int i = 0; i < ring_stages<VT>(); ++i) {
       mbar_init(&ctl->full[i], 1);
       mbar_init(&ctl->empty[i], ConsTeam::kWarps);
     }

@@ -274,6 +274,8 @@ struct alignas(16) ItemDesc {
   int64_t nvec;  // aligned 16-byte vectors from va
 };
 constexpr int kQ = 4;  // queue slots per team
+constexpr int kCapTail = 16384;  // candidates a tail finish on the consumer team resolves in the ring
+static_assert(kCapTail * 8 + 1024 <= kRingBytes && 32768 * 4 + 1024 <= kRingBytes, "ring as scratch");
 constexpr int kSideCandMax = 1 << 17;  // candidate sets the side team resolves itself (else phase B)
 // Batches of fewer rows leave the grid idle at their end, so there every set
 // too large for smem goes to phase B, which resolves it with all CTAs.
@@ -1170,17 +1172,27 @@ struct Engine {
   // far more lines than the sample needs).  All lines are fetched at once by
   // 16-byte asynchronous copies into smem, so the sample costs about one
   // memory round trip and holds no registers while in flight.
+  // With big = true (a whole CTA at the kernel's start, before anything
+  // streams) the ring is the scratch, and rows of 2^23 keys or more take a
+  // larger sample (up to kSampleBig keys: 128 KB of fp32 keys, or 64 KB of
+  // 16-bit ones plus their staging): the threshold then sits closer to the
+  // k-th key, leaving fewer candidates for the row's finish.
   template <class Tm>
-  __device__ uint32_t sample_threshold(const RowCtx& rc) {
-    uint32_t* keys = reinterpret_cast<uint32_t*>(smem);
-    const int S = sample_size(rc.n);
+  __device__ uint32_t sample_threshold(const RowCtx& rc, bool big = false) {
+    uint8_t* scratch = big ? base : smem;
+    uint32_t* keys = reinterpret_cast<uint32_t*>(scratch);
+    int S = sample_size(rc.n);
+    if (big) {
+      constexpr int kSampleBig = ES == 4 ? 32768 : 16384;
+      while (S < kSampleBig && (int64_t)S * 2 * 512 <= rc.n) S *= 2;
+    }
     constexpr int SL = 128 / ES;  // keys per line
     const int nlines = S / SL;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.val_in) + (uintptr_t)rc.in_off * ES;
     const int64_t first = (int64_t)((a + 127) / 128);
     const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 128) - first;  // whole lines in the row
     // fp32 values are converted to keys in place; 16-bit values are staged apart
-    uint8_t* raw = ES == 4 ? smem : smem + kSampleRawOff;
+    uint8_t* raw = ES == 4 ? scratch : big ? scratch + S * 4 + 1024 : smem + kSampleRawOff;
     // line i sits at first + floor(i * (nfull - 1) / (nlines - 1)), stepped in
     // 32.32 fixed point (one division per thread instead of one per line)
     const uint64_t step = nlines > 1 ? ((uint64_t)(nfull - 1) << 32) / (uint64_t)(nlines - 1) : 0;
@@ -1214,7 +1226,7 @@ struct Engine {
     }
     const uint64_t lo = lo32 == 0xFFFFFFFFu && hi32 == 0 ? ~0ull : (uint64_t)lo32, hi = hi32;
     Tm::sync();
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);  // behind the sampled keys
+    uint32_t* hist = reinterpret_cast<uint32_t*>(big ? scratch + S * 4 : smem + kSampleHistOff);  // behind the keys
     const uint32_t t = block_sample_threshold<Tm, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,
                                                          &p.hdr->status);
     Tm::sync();
@@ -1403,8 +1415,8 @@ struct Engine {
 
   // ---- sample item of a pre-filter row: publish the threshold
   template <class Tm>
-  __device__ void sample_item_t(int r, const RowCtx& rc) {
-    const uint32_t T = sample_threshold<Tm>(rc);
+  __device__ void sample_item_t(int r, const RowCtx& rc, bool big = false) {
+    const uint32_t T = sample_threshold<Tm>(rc, big);
     if (Tm::tid() == 0) st_release_u64(&p.rs[r].tready, (1ull << 32) | T);
   }
   __device__ void sample_item(int r, const RowCtx& rc) { sample_item_t<SideTeam>(r, rc); }
@@ -1814,14 +1826,16 @@ struct Engine {
       pos = (int64_t)(uint32_t)e;
     };
     const uint64_t* cand = p.cand + rc.cand_off;
+    // the consumer team finishes in the idle ring (kCapTail entries)
+    constexpr int kCap = Tm::kSize == ConsTeam::kSize ? kCapTail : kCapSB;
     if (rc.kind == kKindGridPref) {
       const int c = m->st_candn;
-      if (c >= rc.k && c <= kCapSB) {
+      if (c >= rc.k && c <= kCap) {
         load_entries<Tm>(ent, cand, c);
         Tm::sync();
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<Tm, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+        smem_resolve<Tm, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kCap * 8), m,
                                 &p.hdr->status);
         smem_emit<Tm, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
         post_process<Tm, VT, SCALE>(p, rc, smem, m);
@@ -2377,7 +2391,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     const RowCtx rc = load_row<VT, SCALE>(p, ir.row);
     if (ir.isA && rc.kind == kKindGridPref) {
       Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
-      e.template sample_item_t<FullTeam>(ir.row, rc);
+      e.template sample_item_t<FullTeam>(ir.row, rc, true);
       first_q = -1;
     }
   }

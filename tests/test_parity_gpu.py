@@ -280,3 +280,15 @@ def test_autotune_keeps_results_exact():
         assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])
     finally:
         rk.autotune_reset()
+
+
+@pytest.mark.parametrize("dist", ["u01", "zipf", "mantissa_noise"])
+@pytest.mark.parametrize("k", [256, 4096])
+def test_single_huge_row(dist, k):
+    """One 2^24-key row: the kernel's first sample is a large one taken by the
+    whole CTA, and the row's finish runs on an idle consumer team."""
+    n = 1 << 24
+    flat = values_for(rk.F32, n, dist, 123)
+    for largest in (True, False):
+        got, want = run_both(flat, [n], k, rk.F32, largest, True)
+        assert_same_selection(got, want, [n], [k], [0], True, f"{dist} largest={largest}")

@@ -1173,10 +1173,10 @@ struct Engine {
   // 16-byte asynchronous copies into smem, so the sample costs about one
   // memory round trip and holds no registers while in flight.
   // With big = true (a whole CTA at the kernel's start, before anything
-  // streams) the ring is the scratch, and rows of 2^23 keys or more take a
-  // larger sample (up to kSampleBig keys: 128 KB of fp32 keys, or 64 KB of
-  // 16-bit ones plus their staging): the threshold then sits closer to the
-  // k-th key, leaving fewer candidates for the row's finish.
+  // streams) the ring is the scratch, and long rows take a larger sample (up
+  // to n / 64 keys and kSampleBig: 128 KB of fp32 keys, or 64 KB of 16-bit
+  // ones plus their staging): the threshold then sits closer to the k-th
+  // key, leaving fewer candidates for the row's finish.
   template <class Tm>
   __device__ uint32_t sample_threshold(const RowCtx& rc, bool big = false) {
     uint8_t* scratch = big ? base : smem;
@@ -1184,7 +1184,7 @@ struct Engine {
     int S = sample_size(rc.n);
     if (big) {
       constexpr int kSampleBig = ES == 4 ? 32768 : 16384;
-      while (S < kSampleBig && (int64_t)S * 2 * 512 <= rc.n) S *= 2;
+      while (S < kSampleBig && (int64_t)S * 2 * 64 <= rc.n) S *= 2;
     }
     constexpr int SL = 128 / ES;  // keys per line
     const int nlines = S / SL;

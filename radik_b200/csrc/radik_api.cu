@@ -239,9 +239,15 @@ size_t zero_bytes(const Layout& L, bool with_hist) { return with_hist ? L.zero_e
 
 // How far A items run ahead of B items beyond what correctness needs.
 // Radix rows re-read their chunks in B items, so their A items run two grids
-// ahead and the re-reads hit L2; pre-filter rows read their chunks once and
-// only need their sample item done, so a short lead suffices.
-int64_t lag_floor(bool has_radix, int grid) { return has_radix ? 2 * (int64_t)grid : std::max(2, grid / 4); }
+// ahead and the re-reads hit L2.  Pre-filter rows read their chunks once and
+// only need their sample item done, so a short lead suffices for fp32; 16-bit
+// rows stream twice the keys per byte, so their start weighs more: there a
+// full grid of samples leads and every CTA opens with a whole-CTA sample
+// (fp16 256 x 2^20, k = 256: +2.4 %; neutral for fp32).
+int64_t lag_floor(bool has_radix, int grid, int dtype) {
+  if (has_radix) return 2 * (int64_t)grid;
+  return dtype == kF32 ? std::max(2, grid / 4) : (int64_t)grid;
+}
 
 // Rows a FIN item trails its row in the B sequence: about one and a half
 // grids of chunk items for uniform rows (their chunks are done by then); a
@@ -364,7 +370,7 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
       maxlag = std::max(maxlag, (r + 1) * una - first_b);
     }
     p.fin_delay = D;
-    p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(has_radix, grid));
+    p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(has_radix, grid, dtype));
   } else {
     std::vector<RowDesc> d(B);
     int64_t off = 0;

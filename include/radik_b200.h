@@ -56,8 +56,8 @@ typedef struct radik_row_desc {
 /* Replaces getRadixSelectLWorkSpaceSize<ValType>(K, n, taskNum, &bytes)
  * (radik/RadixSelect/topk_radixselect.h:22-33): bytes of device workspace for
  * radik_topk() on task_num rows of at most n_max values.  flags must carry
- * RADIK_SORTED if the calls will sort (a larger scratch is reserved for
- * k > 16384). */
+ * RADIK_SORTED if the calls will sort (a merge-sort scratch is reserved for
+ * k > 4096, the outputs a finisher sorts in shared memory). */
 int radik_get_workspace_size(int dtype, uint32_t flags, int K, int n_max, int task_num, size_t* bytes);
 
 /* Replaces topKRadixSelectL<IdxType, LARGEST, ASCEND, WITHSCALE, WITHIDXIN,
@@ -97,19 +97,46 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
  * device_bits (nullable) receives the raw device status word. */
 int radik_get_status(void* workspace, void* stream, int* device_bits);
 
-/* Autotuner (no RadiK counterpart).  Times radik_topk on the caller's
- * buffers with chunk lengths from a quarter to four times the built-in
- * choice (4 runs each, CUDA events, the first discarded) and keeps the
- * fastest for the call's shape bucket -- dtype, sortedness and log2 of the
- * row count, longest row and K -- for every later radik_topk call in this
- * process.  *chunk (nullable) receives the chosen length.  Synchronises the
+/* ---- Autotuner (no RadiK counterpart; RadiK fixes its grid and filter
+ * cache per shape in code, topk_radixselect.h:117-130, 233-258).
+ * A tuned shape bucket -- dtype, form (radik_topk / radik_topk_rows),
+ * sortedness and log2 of the row count, longest row and K -- holds:
+ *   chunk    chunk length (keys) of single-read rows: how a row's work is
+ *            split over the CTAs
+ *   d1       first-digit width of histogram rows (8, 11 or 12 bits)
+ *   cta_cap  rows of up to this many keys (2^15 .. 2^20) are selected by one
+ *            CTA instead of being spread over the grid
+ * A field of 0 keeps the built-in choice.  ms is the tuned call's time in
+ * milliseconds. */
+typedef struct radik_tune_choice {
+  int chunk, d1, cta_cap;
+  float ms;
+} radik_tune_choice;
+
+/* Times radik_topk on the caller's buffers by coordinate descent over the
+ * knobs above (4 runs a candidate, CUDA events, the first discarded) and
+ * keeps the fastest for the call's bucket, for every later call in this
+ * process.  Knobs that cannot change the call are skipped.  Synchronises the
  * stream: do not call it inside a stream capture.  The outputs hold a valid
- * result afterwards.  The environment variable RADIK_CH still overrides. */
+ * result afterwards.  RADIK_CH / RADIK_D1 / RADIK_CTA_CAP still override. */
+int radik_autotune_ex(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                      void* idx_out, void* workspace, size_t workspace_bytes, const int* task_len, int task_num,
+                      int K, void* stream, radik_tune_choice* out);
+/* radik_autotune_ex reporting only the chunk length (nullable). */
 int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
                    void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream,
                    int* chunk);
-/* Forgets every tuned shape. */
+/* The same for radik_topk_rows (device descriptors; the engine's knobs). */
+int radik_autotune_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                        void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                        int task_num, int64_t total_n, int n_max, int k_max, void* stream, radik_tune_choice* out);
+/* Forgets every tuned bucket. */
 void radik_autotune_reset(void);
+/* Writes the tuned buckets to a text file / replaces them with a file's.
+ * A process whose environment names a file in RADIK_TUNE_FILE loads it at
+ * its first call. */
+int radik_autotune_save(const char* path);
+int radik_autotune_load(const char* path);
 
 /* Size of the fixed device scratch behind radik_topk_static(). */
 #define RADIK_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
@@ -140,6 +167,32 @@ void radik_autotune_reset(void);
  *     radik_get_status(*scratch, stream, ...) reads the call's device status. */
 int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
                       void* idx_out, const int* task_len, int task_num, int K, void* stream, void** scratch);
+
+/* ---- One row split over several GPUs (no RadiK counterpart: RadiK selects
+ * each row on one GPU).  Rank r holds a contiguous shard of the row: global
+ * positions [pos_base, pos_base + n) of a row whose positions fit in ib bits
+ * (ib = bits of the row length).  Selection is radix levels over the
+ * composite (selection key << ib | global position), the order a single GPU
+ * uses, so ties go to the lowest global positions.  The caller runs the
+ * levels: every rank histograms the next digit of its shard, the histograms
+ * are summed over the ranks (an all-reduce of 4096 counters), every rank
+ * picks the same bin; when the matched set is small, every rank collects its
+ * certainly-selected and tied keys and the caller gathers them.
+ * radik_b200.sharding.topk_split_row drives both over torch.distributed.
+ * flags: RADIK_LARGEST, RADIK_WITHSCALE (scaler = the row's first value, 0 if
+ * it is NaN or infinite).  Both are asynchronous on the stream. */
+/* hist (device, 4096 counters, cleared here) receives the counts of digit
+ * [w - plen - digit_bits, w - plen) of this shard's composites whose top plen
+ * bits equal prefix, w = key bits (32 for fp32 or scaled rows, else 16) + ib. */
+int radik_shard_histogram(int dtype, uint32_t flags, const void* val_in, int64_t n, int64_t pos_base, int ib,
+                          uint64_t prefix, int plen, int digit_bits, float scaler, uint32_t* hist, void* stream);
+/* Compacts entries (value bits << 32 | global position) of this shard whose
+ * composite's top plen bits are below prefix into better[] and equal to it
+ * into tied[]; counts[0] / counts[1] (device) receive how many there were,
+ * entries past a capacity counted but not stored. */
+int radik_shard_collect(int dtype, uint32_t flags, const void* val_in, int64_t n, int64_t pos_base, int ib,
+                        uint64_t prefix, int plen, float scaler, uint64_t* better, int cap_better, uint64_t* tied,
+                        int cap_tied, uint32_t* counts, void* stream);
 
 /* ---- Serving: a continuous-batching request loop.  No RadiK counterpart:
  * RadiK's callers form their own batches and call topKRadixSelectL once per

@@ -44,6 +44,14 @@ class RowDesc(ctypes.Structure):
     _fields_ = [("in_off", ctypes.c_int64), ("out_off", ctypes.c_int64), ("n", ctypes.c_int32), ("k", ctypes.c_int32)]
 
 
+class TuneChoice(ctypes.Structure):
+    """radik_tune_choice: a tuned bucket's knobs (0: built-in)."""
+    _fields_ = [("chunk", ctypes.c_int), ("d1", ctypes.c_int), ("cta_cap", ctypes.c_int), ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -69,6 +77,12 @@ def lib() -> ctypes.CDLL:
     L.radik_autotune.restype = ctypes.c_int
     L.radik_autotune_reset.argtypes = []
     L.radik_autotune_reset.restype = None
+    L.radik_autotune_ex.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
+                                    ctypes.POINTER(TuneChoice)]
+    L.radik_autotune_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp,
+                                      ctypes.POINTER(TuneChoice)]
+    L.radik_autotune_save.argtypes = [ctypes.c_char_p]
+    L.radik_autotune_load.argtypes = [ctypes.c_char_p]
     L.radik_topk_static.argtypes = [i32, u32, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
                                     ctypes.POINTER(vp)]
     L.radik_strerror.argtypes = [i32]
@@ -77,7 +91,8 @@ def lib() -> ctypes.CDLL:
     L.radik_last_error.restype = ctypes.c_char_p
     L.radik_version.argtypes = []
     for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
-                 "radik_get_status", "radik_version", "radik_topk_static"):
+                 "radik_get_status", "radik_version", "radik_topk_static", "radik_autotune_ex", "radik_autotune_rows",
+                 "radik_autotune_save", "radik_autotune_load"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -126,12 +141,31 @@ def get_rows_workspace_size(dtype: int, task_num: int, total_n: int, n_max: int,
     return out.value
 
 
-def _stream_handle(stream) -> Optional[int]:
+def _stream_handle(stream, device=None) -> Optional[int]:
+    """The raw handle of ``stream``; None means the current stream of
+    ``device`` (the current device when that is None too)."""
     import torch
 
     if stream is None:
-        stream = torch.cuda.current_stream()
+        stream = torch.cuda.current_stream(device)
     return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+def _device_of(t):
+    """A context that makes ``t``'s CUDA device current for the C calls: the
+    library launches on, and looks its static scratch up on, the current
+    device, so a tensor on cuda:1 must not run while cuda:0 is current."""
+    import torch
+
+    if not t.is_cuda:
+        raise RadikError(EINVAL, f"values must be a CUDA tensor (got device {t.device})")
+    return torch.cuda.device(t.device)
+
+
+def _same_device(values, *others) -> None:
+    for o in others:
+        if o is not None and o.device != values.device:
+            raise RadikError(EINVAL, f"tensors on {o.device} and {values.device}: all must be on one device")
 
 
 def topk_radix_select_l(val_in, idx_in, val_out, idx_out, workspace, task_len: Sequence[int], K: int, *,
@@ -151,16 +185,20 @@ def topk_radix_select_l(val_in, idx_in, val_out, idx_out, workspace, task_len: S
     flags = make_flags(largest, need_sorting, ascend, with_scale, with_idx_in, idx64)
     n = len(task_len)
     arr = (ctypes.c_int * max(n, 1))(*[int(x) for x in task_len])
-    _check(lib().radik_topk(
-        dtype_code(val_in.dtype), flags, val_in.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
-        val_out.data_ptr(), idx_out.data_ptr(), workspace.data_ptr(), workspace.numel() * workspace.element_size(),
-        arr, n, int(K), _stream_handle(stream)))
+    _same_device(val_in, idx_in, val_out, idx_out, workspace)
+    with _device_of(val_in):
+        _check(lib().radik_topk(
+            dtype_code(val_in.dtype), flags, val_in.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+            val_out.data_ptr(), idx_out.data_ptr(), workspace.data_ptr(),
+            workspace.numel() * workspace.element_size(), arr, n, int(K), _stream_handle(stream, val_in.device)))
 
 
 def status(workspace, stream=None) -> int:
     """Synchronise ``stream`` and raise RadikError if the last call failed on the device."""
     bits = ctypes.c_int(0)
-    _check(lib().radik_get_status(workspace.data_ptr(), _stream_handle(stream), ctypes.byref(bits)))
+    with _device_of(workspace):
+        _check(lib().radik_get_status(workspace.data_ptr(), _stream_handle(stream, workspace.device),
+                                      ctypes.byref(bits)))
     return bits.value
 
 
@@ -187,15 +225,17 @@ def topk(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bo
     flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
     dt = dtype_code(values.dtype)
     n_max = max(lengths) if lengths else 0
-    if workspace is None:
-        ws_bytes = get_radix_select_l_workspace_size(dt, k, n_max, B, flags)
-        workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=values.device)
-    vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
-    idx = torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device)
-    arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
-    _check(lib().radik_topk(dt, flags, flat.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
-                            vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
-                            arr, B, int(k), _stream_handle(stream)))
+    _same_device(values, idx_in, workspace)
+    with _device_of(values):
+        if workspace is None:
+            ws_bytes = get_radix_select_l_workspace_size(dt, k, n_max, B, flags)
+            workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=values.device)
+        vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
+        idx = torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device)
+        arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
+        _check(lib().radik_topk(dt, flags, flat.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+                                vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                arr, B, int(k), _stream_handle(stream, values.device)))
     if check:
         status(workspace, stream)
     return vals, idx
@@ -232,13 +272,17 @@ def topk_rows(values, rows, *, largest: bool = True, sorted: bool = False, ascen
     total_n, n_max, k_max = bounds
     flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
     dt = dtype_code(values.dtype)
-    if workspace is None:
-        workspace = torch.empty(get_rows_workspace_size(dt, B, total_n, n_max, k_max, flags), dtype=torch.uint8, device=dev)
-    vals = torch.empty(max(total_out, 1), dtype=values.dtype, device=dev)
-    idx = torch.empty(max(total_out, 1), dtype=torch.int64 if idx64 else torch.int32, device=dev)
-    _check(lib().radik_topk_rows(dt, flags, values.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
-                                 vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
-                                 desc.data_ptr(), B, int(total_n), int(n_max), int(k_max), _stream_handle(stream)))
+    _same_device(values, idx_in, workspace, desc)
+    with _device_of(values):
+        if workspace is None:
+            workspace = torch.empty(get_rows_workspace_size(dt, B, total_n, n_max, k_max, flags), dtype=torch.uint8,
+                                    device=dev)
+        vals = torch.empty(max(total_out, 1), dtype=values.dtype, device=dev)
+        idx = torch.empty(max(total_out, 1), dtype=torch.int64 if idx64 else torch.int32, device=dev)
+        _check(lib().radik_topk_rows(dt, flags, values.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
+                                     vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                     desc.data_ptr(), B, int(total_n), int(n_max), int(k_max),
+                                     _stream_handle(stream, dev)))
     if check:
         status(workspace, stream)
     return vals[:total_out], idx[:total_out]
@@ -252,35 +296,58 @@ def topk_static(values, k: int, lengths: Optional[Sequence[int]] = None, *, larg
                 idx64: bool = False, out=None, stream=None, check: bool = True):
     """radik_topk_static: topk() on the library's fixed 32 MiB device scratch.
 
-    The C call allocates nothing; pass ``out=(vals, idx)`` (tensors of B*k
-    slots) to keep this wrapper allocation-free too.  Calls that need more
-    scratch raise RadikError(EWORKSPACE).  Calls in flight at the same time
-    on one device share the scratch and must not overlap.
+    The C call allocates nothing.  To keep this wrapper allocation-free too,
+    pass ``out=(vals, idx)``: contiguous tensors on the values' device with at
+    least B*k elements each, vals of the values' dtype, idx int64 when
+    ``idx64`` else int32.  ``values`` (and ``idx_in``) must then be
+    contiguous: a strided input would need a copy, so it is rejected rather
+    than copied.  Calls that need more scratch raise RadikError(EWORKSPACE).
+    Calls in flight at the same time on one device share the scratch and
+    must not overlap.
     """
     import torch
 
     if values.dim() == 2:
         B, n = values.shape
         lengths = [n] * B
-        flat = values.contiguous().view(-1)
     else:
         if lengths is None:
             lengths = [values.numel()]
-        flat = values.contiguous()
         B = len(lengths)
+    if out is not None:
+        if not values.is_contiguous() or (idx_in is not None and not idx_in.is_contiguous()):
+            raise RadikError(EINVAL, "topk_static with out=: values and idx_in must be contiguous (a copy would "
+                                     "allocate)")
+        vals, idx = out
+        want_idx = torch.int64 if idx64 else torch.int32
+        for name, t, dt_ in (("vals", vals, values.dtype), ("idx", idx, want_idx)):
+            if t.dtype != dt_:
+                raise RadikError(EINVAL, f"topk_static out {name}: dtype {t.dtype}, expected {dt_}")
+            if t.device != values.device:
+                raise RadikError(EINVAL, f"topk_static out {name}: on {t.device}, values on {values.device}")
+            if not t.is_contiguous():
+                raise RadikError(EINVAL, f"topk_static out {name}: must be contiguous")
+            if t.numel() < B * k:
+                raise RadikError(EINVAL, f"topk_static out {name}: {t.numel()} elements, need {B * k}")
+        flat = values
+    else:
+        flat = values.contiguous()
+    _same_device(values, idx_in)
     flags = make_flags(largest, sorted, ascend, with_scale, idx_in is not None, idx64)
-    if out is None:
-        out = (torch.empty((B, k), dtype=values.dtype, device=values.device),
-               torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device))
-    vals, idx = out
     arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
     scratch = ctypes.c_void_p(0)
-    _check(lib().radik_topk_static(dtype_code(values.dtype), flags, flat.data_ptr(),
-                                   idx_in.data_ptr() if idx_in is not None else None, vals.data_ptr(),
-                                   idx.data_ptr(), arr, B, int(k), _stream_handle(stream), ctypes.byref(scratch)))
-    if check and scratch.value:
-        bits = ctypes.c_int(0)
-        _check(lib().radik_get_status(scratch, _stream_handle(stream), ctypes.byref(bits)))
+    with _device_of(values):
+        if out is None:
+            out = (torch.empty((B, k), dtype=values.dtype, device=values.device),
+                   torch.empty((B, k), dtype=torch.int64 if idx64 else torch.int32, device=values.device))
+        vals, idx = out
+        sh = _stream_handle(stream, values.device)
+        _check(lib().radik_topk_static(dtype_code(values.dtype), flags, flat.data_ptr(),
+                                       idx_in.data_ptr() if idx_in is not None else None, vals.data_ptr(),
+                                       idx.data_ptr(), arr, B, int(k), sh, ctypes.byref(scratch)))
+        if check and scratch.value:
+            bits = ctypes.c_int(0)
+            _check(lib().radik_get_status(scratch, sh, ctypes.byref(bits)))
     return vals, idx
 
 
@@ -383,11 +450,12 @@ class Server:
 
 
 def autotune(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bool = True, sorted: bool = False,
-             workspace=None, stream=None) -> int:
-    """radik_autotune: times the chunk-length candidates on these buffers and
-    keeps the fastest for this shape bucket (dtype, sortedness, log2 of rows,
-    longest row, k) for later calls in this process.  Returns the chosen
-    chunk length.  Synchronises ``stream``."""
+             workspace=None, stream=None) -> dict:
+    """radik_autotune_ex: times the knobs of this call's shape bucket (dtype,
+    sortedness, log2 of rows, longest row, k) on these buffers -- the chunk
+    length, the first-digit width and the one-CTA row cap -- and keeps the
+    fastest for later calls in this process.  Returns the choice as a dict
+    (0: the built-in value).  Synchronises ``stream``."""
     import torch
 
     if values.dim() == 2:
@@ -400,16 +468,52 @@ def autotune(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest
         B = len(lengths)
     flags = make_flags(largest, sorted)
     dt = dtype_code(values.dtype)
-    if workspace is None:
-        workspace = torch.empty(get_radix_select_l_workspace_size(dt, k, max(lengths), B, flags), dtype=torch.uint8,
-                                device=values.device)
-    vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
-    idx = torch.empty((B, k), dtype=torch.int32, device=values.device)
-    arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
-    chunk = ctypes.c_int(0)
-    _check(lib().radik_autotune(dt, flags, flat.data_ptr(), None, vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(),
-                                workspace.numel(), arr, B, int(k), _stream_handle(stream), ctypes.byref(chunk)))
-    return chunk.value
+    _same_device(values, workspace)
+    with _device_of(values):
+        if workspace is None:
+            workspace = torch.empty(get_radix_select_l_workspace_size(dt, k, max(lengths), B, flags),
+                                    dtype=torch.uint8, device=values.device)
+        vals = torch.empty((B, k), dtype=values.dtype, device=values.device)
+        idx = torch.empty((B, k), dtype=torch.int32, device=values.device)
+        arr = (ctypes.c_int * max(B, 1))(*[int(x) for x in lengths])
+        choice = TuneChoice()
+        _check(lib().radik_autotune_ex(dt, flags, flat.data_ptr(), None, vals.data_ptr(), idx.data_ptr(),
+                                       workspace.data_ptr(), workspace.numel(), arr, B, int(k),
+                                       _stream_handle(stream, values.device), ctypes.byref(choice)))
+    return choice.as_dict()
+
+
+def autotune_rows(values, desc, B: int, bounds: Tuple[int, int, int], total_out: int, *, largest: bool = True,
+                  sorted: bool = False, workspace=None, stream=None) -> dict:
+    """radik_autotune_rows: the engine's knobs for a radik_topk_rows call
+    (device descriptors ``desc``; bounds = (total_n, n_max, k_max))."""
+    import torch
+
+    total_n, n_max, k_max = bounds
+    flags = make_flags(largest, sorted)
+    dt = dtype_code(values.dtype)
+    with _device_of(values):
+        if workspace is None:
+            workspace = torch.empty(get_rows_workspace_size(dt, B, total_n, n_max, k_max, flags), dtype=torch.uint8,
+                                    device=values.device)
+        vals = torch.empty(max(total_out, 1), dtype=values.dtype, device=values.device)
+        idx = torch.empty(max(total_out, 1), dtype=torch.int32, device=values.device)
+        choice = TuneChoice()
+        _check(lib().radik_autotune_rows(dt, flags, values.data_ptr(), None, vals.data_ptr(), idx.data_ptr(),
+                                         workspace.data_ptr(), workspace.numel(), desc.data_ptr(), B, int(total_n),
+                                         int(n_max), int(k_max), _stream_handle(stream, values.device),
+                                         ctypes.byref(choice)))
+    return choice.as_dict()
+
+
+def autotune_save(path: str) -> None:
+    """Writes the tuned buckets to a text file (RADIK_TUNE_FILE loads it)."""
+    _check(lib().radik_autotune_save(os.fsencode(path)))
+
+
+def autotune_load(path: str) -> None:
+    """Replaces the tuned buckets with a file's."""
+    _check(lib().radik_autotune_load(os.fsencode(path)))
 
 
 def autotune_reset() -> None:

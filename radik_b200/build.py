@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libradik_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in (
     "radik_engine_f32.cu", "radik_engine_f16.cu", "radik_engine_bf16.cu", "radik_plan.cu", "radik_api.cu",
-    "radik_server.cu")]
+    "radik_server.cu", "radik_split.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("radik_common.cuh", "radik_engine.cuh")] + [
     os.path.join(ROOT, "include", "radik_b200.h")]
 OBJ_DIR = os.path.join(ROOT, "_build")
@@ -59,6 +59,8 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
 
     def compile_one(src: str) -> str:
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        if not force and not _stale(obj, [src] + HEADERS + [__file__]):
+            return obj  # up to date: the engine units take minutes each
         cmd = [nvcc, *NVCC_FLAGS, inc, "-c", "-o", obj, src]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
@@ -94,12 +96,22 @@ def build_cli(force: bool = False, verbose: bool = False) -> str:
     return CLI_BIN
 
 
+# Where the build container keeps the reference checkout's radik/ directory
+# (read-only; only the test checker oracle/_ref is built from it).  The GPU
+# runs use the prebuilt oracle/_ref and never read it.
+REFERENCE_SOURCES = os.path.join(os.sep, "root", "reference", "radik")
+
+
 def build_oracle(verbose: bool = False) -> None:
     make = shutil.which("make")
     if make is None:
         raise RuntimeError("make not found")
     out = None if verbose else subprocess.DEVNULL
-    subprocess.run([make, "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True, stdout=out)
+    cmd = [make, "-s", "-C", os.path.join(ROOT, "oracle"), "all"]
+    ref = os.environ.get("RADIK_REF") or (REFERENCE_SOURCES if os.path.isdir(REFERENCE_SOURCES) else "")
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True, stdout=out)
 
 
 def build(force: bool = False, verbose: bool = False) -> None:

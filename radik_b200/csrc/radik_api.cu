@@ -10,6 +10,7 @@
 #include "radik_b200.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -20,9 +21,9 @@
 namespace radik {
 
 cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
-cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
-                        int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
-                        int64_t sort_cap_total, int grid, cudaStream_t stream);
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int cta_cap, int D, uint32_t flags,
+                        RowPlan* plans, int32_t* a_row, int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap,
+                        int64_t cand_cap_total, int64_t sort_cap_total, int grid, cudaStream_t stream);
 cudaError_t engine_max_grid(int dtype, uint32_t flags, int* grid);
 
 namespace {
@@ -43,14 +44,15 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(RADIK_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Cooperative grid of the engine on the current device (one CTA per SM).
+// Cooperative grid of the engine on the current device (one CTA per SM),
+// cached per device and per engine instantiation (value type x WITHSCALE).
 int engine_grid(int dtype, uint32_t flags, int* grid) {
   static std::mutex mu;
-  static int cache[64][2] = {};
+  static int cache[64][6] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  const int key = (flags & kFlagWithScale) ? 1 : 0;
+  const int key = dtype * 2 + ((flags & kFlagWithScale) ? 1 : 0);
   std::lock_guard<std::mutex> lock(mu);
   if (dev >= 0 && dev < 64 && cache[dev][key] > 0) {
     *grid = cache[dev][key];
@@ -108,7 +110,9 @@ Bounds bounds_uniform(int64_t B, int64_t n_max, int64_t K, uint32_t flags) {
   const int64_t nch = std::max<int64_t>(1, ceil_div(n_max, kMinCH));
   b.na = B * nch;
   b.nb = B * (nch + 1);
-  b.cand = n_max > kCtaRowCap ? B * (int64_t)cand_capacity((int32_t)n_max) : 0;
+  // rows above the one-CTA cap keep cand_capacity(n) candidates each; the
+  // cap is tunable down to kCtaRowCapMin
+  b.cand = n_max > kCtaRowCapMin ? B * (int64_t)cand_capacity((int32_t)n_max) : 0;
   const int64_t kk = std::min(n_max, K);
   b.sort = ((flags & kFlagSorted) && kk > kCapSort) ? B * 2 * kk : 0;
   return b;
@@ -130,23 +134,29 @@ int env_int(const char* name, int dflt) {
   return std::atoi(v);
 }
 
-// Tunables: chunk lengths and first-digit width.  Single-read rows use
-// chunks of 4K..256K elements, aiming at about eight chunks per CTA so the
-// work queue balances (the last chunks bound the tail) while each chunk
-// streams long enough to amortise its item overhead; radik_autotune can
-// replace that choice per shape bucket.  Radix rows use 32K-element chunks:
-// their filter items re-read chunks that the histogram items read two grids
-// earlier, and that window (2 x 148 x 128 KB) must stay in L2.  The 12-bit
-// first digit (4096 bins, 16 KB of smem) leaves about n/4096 keys of an
-// i.i.d. row in the selected bin.  RADIK_CH / RADIK_CHR / RADIK_D1 override
-// everything (tuning sweeps).
+// Tunables.  Single-read rows use chunks of 4K..256K elements, aiming at
+// about eight chunks per CTA so the work queue balances (the last chunks
+// bound the tail) while each chunk streams long enough to amortise its item
+// overhead.  Radix rows use 32K-element chunks: their filter items re-read
+// chunks that the histogram items read two grids earlier, and that window
+// (2 x 148 x 128 KB) must stay in L2.  The 12-bit first digit (4096 bins,
+// 16 KB of smem) leaves about n/4096 keys of an i.i.d. row in the selected
+// bin.  Rows of up to 2^18 keys are selected by one CTA.  The autotuner
+// (radik_autotune*) can replace each choice per shape bucket; RADIK_CH /
+// RADIK_CHR / RADIK_D1 / RADIK_CTA_CAP override everything (tuning sweeps).
 struct Config {
-  int CH, CHR, D1;
+  int CH, CHR, D1, cta_cap;
 };
 
-// Autotuned chunk lengths, per shape bucket (radik_autotune).
+// A tuned shape bucket: a field of 0 keeps the built-in choice.
+struct Tuned {
+  int ch = 0;      // chunk length of single-read rows
+  int d1 = 0;      // first-digit width of histogram rows
+  int cta_cap = 0; // rows of up to this many keys go to one CTA
+};
+
 std::mutex g_tune_mu;
-std::map<uint64_t, int> g_tuned_ch;
+std::map<uint64_t, Tuned> g_tuned;
 
 int ilog2(int64_t v) {
   int l = 0;
@@ -165,13 +175,22 @@ uint64_t shape_bucket(int dtype, uint32_t flags, bool rows_form, int64_t B, int6
          ((uint64_t)ilog2(std::max<int64_t>(K, 1)) << 20);
 }
 
-int tuned_ch(uint64_t bucket) {
+void load_tune_file_once();
+
+Tuned tuned_for(uint64_t bucket) {
+  load_tune_file_once();
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  const auto it = g_tuned_ch.find(bucket);
-  return it == g_tuned_ch.end() ? 0 : it->second;
+  const auto it = g_tuned.find(bucket);
+  return it == g_tuned.end() ? Tuned{} : it->second;
 }
 
-Config choose_config(int64_t stream_elems, int grid, uint64_t bucket) {
+int cta_cap_of(const Tuned& t) {
+  const int ecap = env_int("RADIK_CTA_CAP", 0);
+  if (ecap >= kCtaRowCapMin && ecap <= kCtaRowCapMax) return ecap;
+  return t.cta_cap ? t.cta_cap : kCtaRowCap;
+}
+
+Config choose_config(int64_t stream_elems, int grid, const Tuned& t) {
   Config c{};
   const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 8));
   int ch = kMinCH;
@@ -180,10 +199,10 @@ Config choose_config(int64_t stream_elems, int grid, uint64_t bucket) {
   // balance, so no chunk is shorter than 128K keys (single 2^24-key rows:
   // 154 -> 111 us from 8K to 128K chunks).
   if (stream_elems >= ((int64_t)1 << 24)) ch = std::max(ch, 1 << 17);
-  const int tc = tuned_ch(bucket);
-  c.CH = tc ? tc : ch;
+  c.CH = t.ch ? t.ch : ch;
   c.CHR = 32768;
-  c.D1 = kMaxD1;
+  c.D1 = t.d1 ? t.d1 : kMaxD1;
+  c.cta_cap = cta_cap_of(t);
   const int ech = env_int("RADIK_CH", 0);
   if (ech >= kMinCH && ech <= (1 << 24) && (ech % 16) == 0) c.CH = ech;
   const int echr = env_int("RADIK_CHR", 0);
@@ -226,6 +245,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.CH = c.CH;
   p.CHR = c.CHR;
   p.D1 = c.D1;
+  p.cta_cap = c.cta_cap;
   p.S = kSlots;
   p.flags = flags;
   p.spin_limit = kSpinLimit;
@@ -255,9 +275,274 @@ int64_t lag_floor(bool has_radix, int grid, int dtype) {
 constexpr int kFinDelayRows = 64;
 int fin_delay_uniform(int nc, int grid) { return std::max(1, (3 * grid + 2 * std::max(nc, 1) - 1) / (2 * std::max(nc, 1))); }
 
+// A radik_topk call after validation: the engine configuration, the exact
+// item and scratch counts of its rows, and the workspace layout they need.
+struct CallPlan {
+  int B = 0, grid = 0;
+  bool uniform = true, has_radix = false;
+  Config cfg{};
+  int64_t na = 0, nb = 0, cand = 0, sortn = 0;
+  Layout L{};
+};
+
+int plan_call(int dtype, uint32_t flags, const int* task_len, int task_num, int K, CallPlan* cp) {
+  if (!task_len) return fail(RADIK_EINVAL, "radik: task_len is null");
+  const int B = task_num;
+  bool uniform = true;
+  int n_max = 0;
+  for (int i = 0; i < B; ++i) {
+    const int n = task_len[i];
+    if (n < 0) return fail(RADIK_EINVAL, "radik: negative task length");
+    uniform = uniform && n == task_len[0];
+    n_max = std::max(n_max, n);
+  }
+  if ((int64_t)B * K > ((int64_t)1 << 40)) return fail(RADIK_EINVAL, "radik: output too large");
+  const Tuned t = tuned_for(shape_bucket(dtype, flags, false, B, n_max, K));
+  const int cta_cap = cta_cap_of(t);
+  int64_t multi_elems = 0;
+  for (int i = 0; i < B; ++i) {
+    const int kind = row_kind(task_len[i], K, cta_cap);
+    if (kind == kKindAll || kind == kKindGridPref || kind == kKindGridRadix) multi_elems += task_len[i];
+  }
+  int grid = 0;
+  int rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
+  const Config cfg = choose_config(multi_elems, grid, t);
+  int64_t na = 0, nb = 0, cand = 0, sortn = 0;
+  bool has_radix = false;
+  for (int i = 0; i < B; ++i) {
+    const int n = task_len[i];
+    const int kind = row_kind(n, K, cta_cap);
+    has_radix = has_radix || kind == kKindGridRadix;
+    na += row_na(kind, n, cfg.CH, cfg.CHR);
+    nb += row_nbc(kind, n, cfg.CH, cfg.CHR) + row_fin(kind);
+    cand += row_cand_cap(kind, n);
+    const int64_t kk = std::min<int64_t>(n, K);
+    if ((flags & kFlagSorted) && kk > kCapSort) sortn += 2 * kk;
+  }
+  if (na + nb >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many work items");
+  cp->B = B;
+  cp->grid = grid;
+  cp->uniform = uniform;
+  cp->has_radix = has_radix;
+  cp->cfg = cfg;
+  cp->na = na;
+  cp->nb = nb;
+  cp->cand = cand;
+  cp->sortn = sortn;
+  cp->L = make_layout(B, na, nb, cand, sortn);
+  return RADIK_OK;
+}
+
+// Clears the call's state and launches it (planning kernel for uneven
+// lengths, then the engine).  The workspace holds at least cp.L.total bytes.
+int launch_call(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+                uint8_t* ws, const int* task_len, int K, const CallPlan& cp, cudaStream_t stream) {
+  const int B = cp.B, grid = cp.grid;
+  const Config& cfg = cp.cfg;
+  const Layout& L = cp.L;
+  if (!cp.uniform) {
+    // Uneven lengths travel to the device as descriptors copied from host
+    // memory that lives only for this call: a stream capture would record a
+    // copy from freed memory, so it is refused (radik_topk_rows takes device
+    // descriptors and can be captured).
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(stream, &cs);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(RADIK_ENOTSUP, "radik: rows of unequal length cannot be captured in a CUDA graph (their "
+                                 "descriptors are copied from host memory); use radik_topk_rows");
+  }
+  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, cp.has_radix), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
+  if (cp.uniform) {
+    const int n = task_len[0];
+    const int kind = row_kind(n, K, cfg.cta_cap);
+    p.uniform = 1;
+    p.u_n = n;
+    p.u_k = K;
+    p.u_cand_cap = row_cand_cap(kind, n);
+    const int64_t kk = std::min<int64_t>(n, K);
+    p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
+    // B sequence layout (see uniform_b_item) and the lag it needs
+    const int64_t una = row_na(kind, n, cfg.CH, cfg.CHR), nc = row_nbc(kind, n, cfg.CH, cfg.CHR);
+    const int64_t f = row_fin(kind);
+    const int D = fin_delay_uniform((int)nc, grid);
+    const int64_t Dd = std::min<int64_t>(D, B);
+    auto b0 = [&](int64_t q) { return q < Dd ? q * nc : Dd * nc + (q - Dd) * (nc + f); };
+    int64_t maxlag = 0;
+    for (int64_t r = 0; r < B && (nc > 0 || f); ++r) {
+      int64_t first_b;
+      if (nc > 0) first_b = b0(r);
+      else first_b = (r + Dd < B) ? b0(r + Dd) + nc : (int64_t)B * nc + f * (B - Dd) + (r - (B - Dd));
+      maxlag = std::max(maxlag, (r + 1) * una - first_b);
+    }
+    p.fin_delay = D;
+    p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(cp.has_radix, grid, dtype));
+  } else {
+    std::vector<RowDesc> d(B);
+    int64_t off = 0;
+    for (int i = 0; i < B; ++i) {
+      d[i].in_off = off;
+      d[i].out_off = (int64_t)i * K;
+      d[i].n = task_len[i];
+      d[i].k = K;
+      off += task_len[i];
+    }
+    RowDesc* dd = reinterpret_cast<RowDesc*>(ws + L.descs);
+    // pageable source: the copy is staged before this call returns
+    e = cudaMemcpyAsync(dd, d.data(), sizeof(RowDesc) * B, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
+    p.a_row = reinterpret_cast<int32_t*>(ws + L.a_row);
+    p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
+    e = launch_plan(dd, B, cfg.CH, cfg.CHR, cfg.cta_cap, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
+                    reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, cp.na,
+                    cp.nb, cp.cand, cp.sortn, grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "plan launch");
+  }
+  e = launch_engine(dtype, p, grid, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+  return RADIK_OK;
+}
+
 // Workspace of radik_topk_static(): static device memory of this module, one
 // copy per device the module is loaded on.
 static __device__ __align__(256) unsigned char g_static_scratch[RADIK_STATIC_SCRATCH_BYTES];
+
+// Times one call of fn (4 runs, the first discarded) with CUDA events on
+// the stream; returns RADIK_OK and the summed milliseconds of three runs.
+template <typename Fn>
+int time_call(cudaStream_t stream, cudaEvent_t a, cudaEvent_t b, Fn&& fn, float* ms_sum) {
+  *ms_sum = 0.f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(a, stream);
+    const int rc = fn();
+    cudaEventRecord(b, stream);
+    if (rc != RADIK_OK) return rc;
+    if (cudaEventSynchronize(b) != cudaSuccess) return fail(RADIK_ECUDA, "cudaEventSynchronize");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0) *ms_sum += ms;
+  }
+  return RADIK_OK;
+}
+
+// Coordinate descent over a bucket's knobs: each candidate value of a knob
+// is timed with the others at their best so far; the fastest is kept.  The
+// bucket's entry is live while it is timed (the calls read it), and holds
+// the winner afterwards.  Knobs whose candidates cannot change the call are
+// skipped (no histogram row, no row in the CTA-cap range).
+template <typename Call>
+int tune_bucket(uint64_t bucket, cudaStream_t stream, bool has_radix, bool cap_matters, int ch_default, Call&& call,
+                radik_tune_choice* out) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return fail(RADIK_ECUDA, "cudaEventCreate");
+  auto set = [&](const Tuned& t) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[bucket] = t;
+  };
+  Tuned best{};
+  float best_ms = 1e30f;
+  int rc = RADIK_OK;
+  auto trial = [&](const Tuned& t) {
+    if (rc != RADIK_OK) return;
+    set(t);
+    float ms = 0.f;
+    rc = time_call(stream, a, b, call, &ms);
+    if (rc == RADIK_OK && ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  };
+  trial(best);  // the built-in choice
+  // 1. chunk length of single-read rows: a quarter to four times the pick
+  {
+    const Tuned base = best;
+    for (int ch = std::max(kMinCH, ch_default / 4); ch <= std::min(kMaxCH, ch_default * 4); ch *= 2) {
+      Tuned t = base;
+      t.ch = ch;
+      trial(t);
+    }
+  }
+  // 2. first-digit width of histogram rows
+  if (has_radix) {
+    const Tuned base = best;
+    for (int d1 : {8, 11}) {
+      Tuned t = base;
+      t.d1 = d1;
+      trial(t);
+    }
+  }
+  // 3. the one-CTA row cap
+  if (cap_matters) {
+    const Tuned base = best;
+    for (int cap = kCtaRowCapMin; cap <= kCtaRowCapMax; cap *= 2) {
+      if (cap == kCtaRowCap) continue;
+      Tuned t = base;
+      t.cta_cap = cap;
+      trial(t);
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (rc == RADIK_OK) g_tuned[bucket] = best;
+    else g_tuned.erase(bucket);
+  }
+  if (rc != RADIK_OK) return rc;
+  if (out) {
+    out->chunk = best.ch;
+    out->d1 = best.d1;
+    out->cta_cap = best.cta_cap;
+    out->ms = best_ms / 3.f;
+  }
+  return RADIK_OK;
+}
+
+// The tuning table as text: one bucket per line, "key ch d1 cta_cap".
+std::once_flag g_tune_file_once;
+
+int load_tune_table(const char* path, bool replace) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return fail(RADIK_EINVAL, std::string("radik: cannot read tuning table ") + path);
+  std::map<uint64_t, Tuned> m;
+  char line[256];
+  int bad = 0;
+  while (std::fgets(line, sizeof line, f)) {
+    if (line[0] == '#' || line[0] == '\n') continue;
+    unsigned long long key = 0;
+    Tuned t;
+    if (std::sscanf(line, "%llx %d %d %d", &key, &t.ch, &t.d1, &t.cta_cap) != 4) {
+      ++bad;
+      continue;
+    }
+    const bool ok = (t.ch == 0 || (t.ch >= kMinCH && t.ch <= kMaxCH && t.ch % 16 == 0)) &&
+                    (t.d1 == 0 || (t.d1 >= kMinD1 && t.d1 <= kMaxD1)) &&
+                    (t.cta_cap == 0 || (t.cta_cap >= kCtaRowCapMin && t.cta_cap <= kCtaRowCapMax));
+    if (!ok) {
+      ++bad;
+      continue;
+    }
+    m[(uint64_t)key] = t;
+  }
+  std::fclose(f);
+  if (bad) return fail(RADIK_EINVAL, std::string("radik: malformed lines in tuning table ") + path);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  if (replace) g_tuned.clear();
+  for (const auto& kv : m) g_tuned[kv.first] = kv.second;
+  return RADIK_OK;
+}
+
+// RADIK_TUNE_FILE names a table that the first call in the process loads.
+void load_tune_file_once() {
+  std::call_once(g_tune_file_once, [] {
+    const char* path = std::getenv("RADIK_TUNE_FILE");
+    if (path && *path) load_tune_table(path, false);
+  });
+}
 
 }  // namespace
 }  // namespace radik
@@ -308,92 +593,12 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
   if (rc) return rc;
   if (task_num < 0 || K < 0) return fail(RADIK_EINVAL, "radik: negative task_num or K");
   if (task_num == 0 || K == 0) return RADIK_OK;
-  if (!task_len) return fail(RADIK_EINVAL, "radik: task_len is null");
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-  const int B = task_num;
-  bool uniform = true;
-  int64_t multi_elems = 0;
-  for (int i = 0; i < B; ++i) {
-    const int n = task_len[i];
-    if (n < 0) return fail(RADIK_EINVAL, "radik: negative task length");
-    uniform = uniform && n == task_len[0];
-    const int kind = row_kind(n, K);
-    if (kind == kKindAll || kind == kKindGridPref || kind == kKindGridRadix) multi_elems += n;
-  }
-  if ((int64_t)B * K > ((int64_t)1 << 40)) return fail(RADIK_EINVAL, "radik: output too large");
-  int grid = 0;
-  rc = engine_grid(dtype, flags, &grid);
+  CallPlan cp;
+  rc = plan_call(dtype, flags, task_len, task_num, K, &cp);
   if (rc) return rc;
-  int n_max_call = 0;
-  for (int i = 0; i < B; ++i) n_max_call = std::max(n_max_call, task_len[i]);
-  const Config cfg = choose_config(multi_elems, grid, shape_bucket(dtype, flags, false, B, n_max_call, K));
-  // exact needs of this call
-  int64_t na = 0, nb = 0, cand = 0, sortn = 0;
-  bool has_radix = false;
-  for (int i = 0; i < B; ++i) {
-    const int n = task_len[i];
-    const int kind = row_kind(n, K);
-    has_radix = has_radix || kind == kKindGridRadix;
-    na += row_na(kind, n, cfg.CH, cfg.CHR);
-    nb += row_nbc(kind, n, cfg.CH, cfg.CHR) + row_fin(kind);
-    cand += row_cand_cap(kind, n);
-    const int64_t kk = std::min<int64_t>(n, K);
-    if ((flags & kFlagSorted) && kk > kCapSort) sortn += 2 * kk;
-  }
-  if (na + nb >= ((int64_t)1 << 30)) return fail(RADIK_EINVAL, "radik: too many work items");
-  const Layout L = make_layout(B, na, nb, cand, sortn);
-  if (workspace_bytes < L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
-  uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, has_radix), stream);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-  EngineParams p = base_params(val_in, idx_in, val_out, idx_out, ws, L, B, cfg, flags);
-  if (uniform) {
-    const int n = task_len[0];
-    const int kind = row_kind(n, K);
-    p.uniform = 1;
-    p.u_n = n;
-    p.u_k = K;
-    p.u_cand_cap = row_cand_cap(kind, n);
-    const int64_t kk = std::min<int64_t>(n, K);
-    p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
-    // B sequence layout (see uniform_b_item) and the lag it needs
-    const int64_t una = row_na(kind, n, cfg.CH, cfg.CHR), nc = row_nbc(kind, n, cfg.CH, cfg.CHR);
-    const int64_t f = row_fin(kind);
-    const int D = fin_delay_uniform((int)nc, grid);
-    const int64_t Dd = std::min<int64_t>(D, B);
-    auto b0 = [&](int64_t q) { return q < Dd ? q * nc : Dd * nc + (q - Dd) * (nc + f); };
-    int64_t maxlag = 0;
-    for (int64_t r = 0; r < B && (nc > 0 || f); ++r) {
-      int64_t first_b;
-      if (nc > 0) first_b = b0(r);
-      else first_b = (r + Dd < B) ? b0(r + Dd) + nc : (int64_t)B * nc + f * (B - Dd) + (r - (B - Dd));
-      maxlag = std::max(maxlag, (r + 1) * una - first_b);
-    }
-    p.fin_delay = D;
-    p.lag = (int32_t)std::max<int64_t>(maxlag + 1, lag_floor(has_radix, grid, dtype));
-  } else {
-    std::vector<RowDesc> d(B);
-    int64_t off = 0;
-    for (int i = 0; i < B; ++i) {
-      d[i].in_off = off;
-      d[i].out_off = (int64_t)i * K;
-      d[i].n = task_len[i];
-      d[i].k = K;
-      off += task_len[i];
-    }
-    RowDesc* dd = reinterpret_cast<RowDesc*>(ws + L.descs);
-    e = cudaMemcpyAsync(dd, d.data(), sizeof(RowDesc) * B, cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
-    p.plans = reinterpret_cast<RowPlan*>(ws + L.plans);
-    p.a_row = reinterpret_cast<int32_t*>(ws + L.a_row);
-    p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
-    e = launch_plan(dd, B, cfg.CH, cfg.CHR, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans), reinterpret_cast<int32_t*>(ws + L.a_row),
-                    reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, na, nb, cand, sortn, grid, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "plan launch");
-  }
-  e = launch_engine(dtype, p, grid, stream);
-  if (e != cudaSuccess) return cuda_fail(e, "engine launch");
-  return RADIK_OK;
+  if (workspace_bytes < cp.L.total) return fail(RADIK_EWORKSPACE, "radik: workspace too small");
+  return launch_call(dtype, flags, val_in, idx_in, val_out, idx_out, static_cast<uint8_t*>(workspace), task_len, K,
+                     cp, static_cast<cudaStream_t>(stream_));
 }
 
 int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
@@ -414,7 +619,7 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  const Config cfg = choose_config(total_n, grid, shape_bucket(dtype, flags, true, B, n_max, k_max));
+  const Config cfg = choose_config(total_n, grid, tuned_for(shape_bucket(dtype, flags, true, B, n_max, k_max)));
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, true), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -424,7 +629,7 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   p.b_row = reinterpret_cast<int32_t*>(ws + L.b_row);
   // The item budget assumed kMinCH-long chunks; with the chosen CH the true
   // count is smaller, so the bound still holds.
-  e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, cfg.CHR, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
+  e = launch_plan(reinterpret_cast<const RowDesc*>(rows), B, cfg.CH, cfg.CHR, cfg.cta_cap, kFinDelayRows, flags, reinterpret_cast<RowPlan*>(ws + L.plans),
                   reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, b.na, b.nb,
                   b.cand, b.sort, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan launch");
@@ -449,9 +654,9 @@ int radik_get_status(void* workspace, void* stream_, int* device_bits) {
   return RADIK_OK;
 }
 
-int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
-                   void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream_,
-                   int* chunk) {
+int radik_autotune_ex(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                      void* idx_out, void* workspace, size_t workspace_bytes, const int* task_len, int task_num,
+                      int K, void* stream_, radik_tune_choice* out) {
   if (task_num <= 0 || K <= 0 || !task_len) return fail(RADIK_EINVAL, "radik_autotune: empty call");
   int n_max = 0;
   int64_t total = 0;
@@ -464,74 +669,113 @@ int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* id
   int rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
   const uint64_t bucket = shape_bucket(dtype, flags, false, task_num, n_max, K);
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-  cudaEvent_t a = nullptr, b = nullptr;
-  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return fail(RADIK_ECUDA, "cudaEventCreate");
-  // candidates: powers of two from a quarter to four times the default's pick
-  const Config dflt = choose_config(total, grid, ~0ull);
-  int best = 0;
-  float best_ms = 1e30f;
-  for (int ch = std::max(kMinCH, dflt.CH / 4); ch <= std::min(kMaxCH, dflt.CH * 4); ch *= 2) {
-    {
-      std::lock_guard<std::mutex> lock(g_tune_mu);
-      g_tuned_ch[bucket] = ch;
-    }
-    float ms_sum = 0.f;
-    for (int rep = 0; rep < 4 && rc == RADIK_OK; ++rep) {
-      cudaEventRecord(a, stream);
-      rc = radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes, task_len, task_num,
-                      K, stream_);
-      cudaEventRecord(b, stream);
-      if (rc == RADIK_OK && cudaEventSynchronize(b) != cudaSuccess) rc = fail(RADIK_ECUDA, "cudaEventSynchronize");
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, a, b);
-      if (rep > 0) ms_sum += ms;  // the first run warms up
-    }
-    if (rc != RADIK_OK) break;
-    if (ms_sum < best_ms) {
-      best_ms = ms_sum;
-      best = ch;
-    }
+  bool has_radix = false, cap_matters = false;
+  for (int i = 0; i < task_num; ++i) {
+    const int n = task_len[i];
+    has_radix = has_radix || row_kind(n, K, kCtaRowCapMax) == kKindGridRadix ||
+                row_kind(n, K, kCtaRowCapMin) == kKindGridRadix;
+    cap_matters = cap_matters || (n > kCtaRowCapMin && n <= kCtaRowCapMax && K < n);
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  {
-    std::lock_guard<std::mutex> lock(g_tune_mu);
-    if (best) g_tuned_ch[bucket] = best;
-    else g_tuned_ch.erase(bucket);
-  }
+  const Config dflt = choose_config(total, grid, Tuned{});
+  rc = tune_bucket(bucket, static_cast<cudaStream_t>(stream_), has_radix, cap_matters, dflt.CH,
+                   [&] {
+                     return radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes,
+                                       task_len, task_num, K, stream_);
+                   },
+                   out);
   if (rc != RADIK_OK) return rc;
-  if (chunk) *chunk = best;
+  return radik_get_status(workspace, stream_, nullptr);
+}
+
+int radik_autotune(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out, void* idx_out,
+                   void* workspace, size_t workspace_bytes, const int* task_len, int task_num, int K, void* stream_,
+                   int* chunk) {
+  radik_tune_choice c{};
+  const int rc = radik_autotune_ex(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes,
+                                   task_len, task_num, K, stream_, &c);
+  if (rc == RADIK_OK && chunk) *chunk = c.chunk;
+  return rc;
+}
+
+int radik_autotune_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                        void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                        int task_num, int64_t total_n, int n_max, int k_max, void* stream_, radik_tune_choice* out) {
+  if (task_num <= 0 || !rows) return fail(RADIK_EINVAL, "radik_autotune_rows: empty call");
+  int grid = 0;
+  int rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
+  const uint64_t bucket = shape_bucket(dtype, flags, true, task_num, n_max, k_max);
+  // the rows live on the device: every knob is tried
+  const Config dflt = choose_config(total_n, grid, Tuned{});
+  rc = tune_bucket(bucket, static_cast<cudaStream_t>(stream_), true, n_max > kCtaRowCapMin, dflt.CH,
+                   [&] {
+                     return radik_topk_rows(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes,
+                                            rows, task_num, total_n, n_max, k_max, stream_);
+                   },
+                   out);
+  if (rc != RADIK_OK) return rc;
   return radik_get_status(workspace, stream_, nullptr);
 }
 
 void radik_autotune_reset(void) {
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  g_tuned_ch.clear();
+  g_tuned.clear();
+}
+
+int radik_autotune_save(const char* path) {
+  if (!path) return fail(RADIK_EINVAL, "radik_autotune_save: path is null");
+  std::map<uint64_t, Tuned> m;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    m = g_tuned;
+  }
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(RADIK_EINVAL, std::string("radik: cannot write tuning table ") + path);
+  std::fprintf(f, "# radik_b200 tuning table: bucket chunk d1 cta_cap (0: built-in)\n");
+  std::fprintf(f, "# bucket = dtype | rows_form << 2 | sorted << 3 | log2(rows) << 4 | log2(n_max) << 12 | "
+                  "log2(k) << 20\n");
+  for (const auto& kv : m)
+    std::fprintf(f, "%llx %d %d %d\n", (unsigned long long)kv.first, kv.second.ch, kv.second.d1,
+                 kv.second.cta_cap);
+  const bool ok = std::fclose(f) == 0;
+  return ok ? RADIK_OK : fail(RADIK_EINVAL, std::string("radik: cannot write tuning table ") + path);
+}
+
+int radik_autotune_load(const char* path) {
+  if (!path) return fail(RADIK_EINVAL, "radik_autotune_load: path is null");
+  load_tune_file_once();
+  return load_tune_table(path, true);
 }
 
 int radik_topk_static(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
                       void* idx_out, const int* task_len, int task_num, int K, void* stream, void** scratch) {
   if (scratch) *scratch = nullptr;
+  // validated with a stand-in workspace: the array's address is looked up
+  // only once the call is known to fit
+  int rc = check_common(dtype, flags, val_in, idx_in, val_out, idx_out, reinterpret_cast<void*>(uintptr_t(256)));
+  if (rc) return rc;
+  if (task_num < 0 || K < 0) return fail(RADIK_EINVAL, "radik: negative task_num or K");
+  CallPlan cp;
+  if (task_num > 0 && K > 0) {
+    rc = plan_call(dtype, flags, task_len, task_num, K, &cp);
+    if (rc) return rc;
+    if (cp.L.total > RADIK_STATIC_SCRATCH_BYTES) {
+      int n_max = 0;
+      for (int i = 0; i < task_num; ++i) n_max = std::max(n_max, task_len[i]);
+      return fail(RADIK_EWORKSPACE, "radik_topk_static: " + std::to_string(task_num) + " rows of up to " +
+                                        std::to_string(n_max) + " values with K = " + std::to_string(K) + " need " +
+                                        std::to_string(cp.L.total) + " bytes of scratch, more than the " +
+                                        std::to_string(RADIK_STATIC_SCRATCH_BYTES) +
+                                        "-byte static array; call radik_topk with a caller-owned workspace");
+    }
+  }
   void* ws = nullptr;
   const cudaError_t e = cudaGetSymbolAddress(&ws, g_static_scratch);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
   if (scratch) *scratch = ws;
-  const int rc = radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, ws, RADIK_STATIC_SCRATCH_BYTES, task_len,
-                            task_num, K, stream);
-  // ws is non-null and aligned, so RADIK_EWORKSPACE can only mean too small
-  if (rc == RADIK_EWORKSPACE) {
-    int n_max = 0;
-    for (int i = 0; i < task_num; ++i) n_max = std::max(n_max, task_len[i]);
-    size_t need = 0;
-    radik_get_workspace_size(dtype, flags, K, n_max, task_num, &need);
-    return fail(RADIK_EWORKSPACE, "radik_topk_static: " + std::to_string(task_num) + " rows of up to " +
-                                      std::to_string(n_max) + " values with K = " + std::to_string(K) +
-                                      " need up to " + std::to_string(need) + " bytes of scratch, more than the " +
-                                      std::to_string(RADIK_STATIC_SCRATCH_BYTES) +
-                                      "-byte static array; call radik_topk with a caller-owned workspace");
-  }
-  return rc;
+  if (task_num == 0 || K == 0) return RADIK_OK;
+  return launch_call(dtype, flags, val_in, idx_in, val_out, idx_out, static_cast<uint8_t*>(ws), task_len, K, cp,
+                     static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

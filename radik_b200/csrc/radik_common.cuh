@@ -38,7 +38,9 @@ constexpr int kCtasPerSM = 1;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCapSB = 6144;             // candidates a finisher resolves in smem (48 KB)
 constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
-constexpr int kCtaRowCap = 1 << 18;      // rows this short are selected by one CTA
+constexpr int kCtaRowCap = 1 << 18;      // default: rows this short are selected by one CTA
+constexpr int kCtaRowCapMin = 1 << 15;   // range of the tunable one-CTA row cap
+constexpr int kCtaRowCapMax = 1 << 20;
 constexpr int kCapSort = 4096;           // outputs a finisher sorts in smem (32 KB)
 constexpr int kMaxD1 = 12;               // widest first digit (16 KB smem hist)
 constexpr int kMinD1 = 8;
@@ -54,7 +56,7 @@ constexpr int kMiscBytes = 4096;         // tail of smem for scalars / scan scra
 enum : int32_t {
   kKindEmpty = 0,      // k <= 0: nothing to do
   kKindSmem = 1,       // n <= kSmemRowCap: one item, row held in smem
-  kKindCta = 2,        // n <= kCtaRowCap: one item, one CTA selects the row
+  kKindCta = 2,        // n <= cta_cap (kCtaRowCap by default): one item, one CTA selects the row
   kKindAll = 3,        // k >= n: chunk items copy the whole row
   kKindGridPref = 4,   // large row, small k/n: sample item + filter chunks
   kKindGridRadix = 5,  // large row, large k/n: histogram chunks + filter chunks
@@ -75,7 +77,6 @@ enum : int32_t {
   kStatusTimeout = 1,       // a bounded wait gave up
   kStatusSelect = 2,        // a histogram did not hold k keys (internal)
   kStatusCapacity = 4,      // workspace too small for the planned rows
-  kStatusOverflow = 8,      // a candidate region overflowed (internal)
   kStatusLevels = 16,       // resolution did not converge (internal)
 };
 
@@ -168,6 +169,7 @@ struct EngineParams {
   int32_t CH;               // chunk length of single-read rows (elements), multiple of 16
   int32_t CHR;              // chunk length of radix rows (elements), multiple of 16
   int32_t D1;               // first digit width of histogram rows
+  int32_t cta_cap;          // rows of up to this many keys are selected by one CTA
   int32_t S;                // hist ring slots
   int32_t lag;              // uniform mode: A-ahead-of-B distance
   int32_t fin_delay;        // uniform mode: rows a FIN item trails its row
@@ -195,11 +197,12 @@ __host__ __device__ inline int index_bits(int64_t n) {
   return b;
 }
 __host__ __device__ inline bool is_smem_row(int32_t n) { return n <= kSmemRowCap; }
-__host__ __device__ inline int row_kind(int32_t n, int32_t k) {
+// cta_cap: rows of up to this many keys are selected by one CTA (tunable).
+__host__ __device__ inline int row_kind(int32_t n, int32_t k, int32_t cta_cap) {
   if (k <= 0) return kKindEmpty;
   if (n <= kSmemRowCap) return kKindSmem;
   if (k >= n) return kKindAll;
-  if (n <= kCtaRowCap) return kKindCta;
+  if (n <= cta_cap) return kKindCta;
   if ((int64_t)k * kPrefRatio <= (int64_t)n) return kKindGridPref;
   return kKindGridRadix;
 }

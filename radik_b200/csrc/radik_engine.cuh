@@ -49,6 +49,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <mutex>
+
 namespace radik {
 namespace dev {
 
@@ -280,6 +282,7 @@ constexpr int kSideCandMax = 1 << 17;  // candidate sets the side team resolves 
 // Batches of fewer rows leave the grid idle at their end, so there every set
 // too large for smem goes to phase B, which resolves it with all CTAs.
 constexpr int kSideResolveMinRows = 32;
+
 struct Ctrl {
   uint64_t full[kStages];   // ring slot filled
   uint64_t empty[kStages];  // ring slot drained by every consumer warp
@@ -458,7 +461,7 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
     c.k = p.u_k;
     c.in_off = (int64_t)r * p.u_n;
     c.out_off = (int64_t)r * p.u_k;
-    c.kind = row_kind(c.n, c.k);
+    c.kind = row_kind(c.n, c.k, p.cta_cap);
     c.na = row_na(c.kind, c.n, p.CH, p.CHR);
     c.nbc = row_nbc(c.kind, c.n, p.CH, p.CHR);
     c.a0 = r * c.na;
@@ -475,7 +478,7 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
     c.sort_off = pl.sort_off;
     c.n = pl.n;
     c.k = pl.k;
-    c.kind = row_kind(c.n, c.k);
+    c.kind = row_kind(c.n, c.k, p.cta_cap);
     c.na = row_na(c.kind, c.n, p.CH, p.CHR);
     c.nbc = row_nbc(c.kind, c.n, p.CH, p.CHR);
     c.a0 = pl.a0;
@@ -632,16 +635,17 @@ __device__ __forceinline__ void flush_out(const EngineParams& p, const WarpBuf& 
   }
 }
 
-// Flushes a warp buffer to a candidate region of capacity cap.
-__device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint64_t* dst, int32_t cap,
-                                           int32_t* status) {
+// Flushes a warp buffer to a candidate region of capacity cap.  Entries past
+// the capacity are dropped but still counted, so the reader sees the true
+// count and takes its fallback (a pre-filter row whose threshold let more
+// than cand_cap keys through is resolved over the row itself in phase B).
+__device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint64_t* dst, int32_t cap) {
   const unsigned lane = threadIdx.x & 31u;
   uint32_t base = 0;
   if (lane == 0) base = atomicAdd(ctr, s.n);
   base = __shfl_sync(kFull, base, 0);
   for (uint32_t i = lane; i < s.n; i += 32)
     if (base + i < (uint32_t)cap) dst[base + i] = s.buf[i];
-  (void)status;
 }
 
 // ----------------------------------------------------------------------------
@@ -1020,11 +1024,14 @@ template <class Tm>
 __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
   // bar_count only grows during a call (the header is cleared per call):
   // every CTA takes the barriers in the same order, so barrier b completes at
-  // (b + 1) * gridDim.x arrivals -- one atomic per CTA, then a poll.
+  // (b + 1) * gridDim.x arrivals -- one atomic per CTA, then a poll.  The
+  // arrival is a release at GPU scope (it orders the CTA's writes, gathered
+  // by the team barrier before it) and the poll an acquire; a sequentially
+  // consistent fence on each side cost about 8 us per barrier on B200.
   Tm::sync();
   if (Tm::tid() == 0) {
-    __threadfence();
-    const uint32_t old = atomicAdd(&h->bar_count, 1u);
+    uint32_t old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&h->bar_count) : "memory");
     const uint32_t target = (old / gridDim.x + 1u) * gridDim.x;
     uint32_t it = 0;
     while (ld_acquire(&h->bar_count) < target) {
@@ -1034,7 +1041,6 @@ __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
       }
       __nanosleep(32);
     }
-    __threadfence();
   }
   Tm::sync();
 }
@@ -1258,9 +1264,10 @@ struct Engine {
     post_process<SideTeam, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
   }
 
-  // ---- one CTA, the whole row from global memory (n <= kCtaRowCap)
+  // ---- one CTA, the whole row from global memory (n <= p.cta_cap)
   // Pass over the row classifying by a composite prefix; to_out hits go to
   // the output, to_ent hits into the smem entry array (cap kCapSB).
+  template <class Tm = SideTeam>
   __device__ void cta_filter(const RowCtx& rc, RowState* rs, uint64_t prefix, int plen, bool final_mode,
                              uint64_t* ent) {
     const int W = K::KB + rc.IB;
@@ -1280,7 +1287,7 @@ struct Engine {
       const uint32_t se = warp_reserve(to_ent ? 1u : 0u, &m->counter);
       if (to_ent && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
     };
-    for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+    for_range_v<Tm, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
       for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
     });
@@ -1470,7 +1477,7 @@ struct Engine {
         const uint32_t tot = __shfl_sync(kFull, h, src);
         if (cb.n + tot > (uint32_t)kCap) {
           __syncwarp();
-          flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+          flush_cand(cb, ctr, dst, rc.cand_cap);
           cb.n = 0;
           __syncwarp();
         }
@@ -1493,7 +1500,7 @@ struct Engine {
       const uint32_t tot = __shfl_sync(kFull, x, 31);
       if (cb.n + tot > (uint32_t)kCap) {
         __syncwarp();
-        flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+        flush_cand(cb, ctr, dst, rc.cand_cap);
         cb.n = 0;
         __syncwarp();
       }
@@ -1560,7 +1567,7 @@ struct Engine {
             push(hm, 0u, [&](int e) { return vec_elem<ES>(x, e); }, pos0);
           }
         });
-    if (cb.n) flush_cand(cb, ctr, dst, rc.cand_cap, &p.hdr->status);
+    if (cb.n) flush_cand(cb, ctr, dst, rc.cand_cap);
     defer_release(r);
   }
 
@@ -1602,19 +1609,22 @@ struct Engine {
         if (v.w) atomicAdd(ghist + i + 3, v.w);
       }
     }
-    __threadfence();
+    // The team's histogram atomics precede the count (team barrier, then one
+    // fence on each side of it by the counting thread).
     ConsTeam::sync();
     RowState* rs = p.rs + r;
-    if (ConsTeam::tid() == 0) m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
+    if (ConsTeam::tid() == 0) {
+      __threadfence();
+      m->bcast2 = atomicAdd(&rs->hticket, 1) == rc.na - 1;
+      __threadfence();
+    }
     ConsTeam::sync();
     if (!m->bcast2) return;
     // Last histogram item of the row: select the first digit's bin.
-    __threadfence();
     block_select<ConsTeam, true>(ghist, NB, (uint32_t)rc.k, m);
     const bool found = m->sel_found != 0;
     const uint32_t bin = m->sel_bin, cum = m->sel_cum, cnt = m->sel_cnt;
     for (int i = ConsTeam::tid() * 4; i < NB; i += ConsTeam::kSize * 4) *reinterpret_cast<uint4*>(ghist + i) = make_uint4(0, 0, 0, 0);
-    __threadfence();
     ConsTeam::sync();
     if (ConsTeam::tid() == 0) {
       int mode;
@@ -1663,7 +1673,7 @@ struct Engine {
       uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->cand_count);
       uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
       uint64_t* dst = p.cand + rc.cand_off;
-      auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, rc.cand_cap, &p.hdr->status); };
+      auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, rc.cand_cap); };
       auto flo = [&](const WarpBuf& s) { flush_out<VT>(p, s, octr, rc.out_off, rc.k); };
       const uint32_t flip = rc.flip;
       const float sc = rc.scaler;
@@ -1809,7 +1819,8 @@ struct Engine {
   __device__ void finish_row(int r) {
     const RowCtx rc = load_row<VT, SCALE>(p, r);
     RowState* rs = p.rs + r;
-    __threadfence();
+    // thread 0 of the team acquired the row's chunk counter (fin_item_t) and
+    // the team barrier there passed that on: the row's state is visible
     if (Tm::tid() == 0) {
       m->st_mode = rc.kind == kKindAll ? kModeAll : __ldcg(&rs->mode);
       m->st_krem = __ldcg(&rs->krem);
@@ -1829,8 +1840,11 @@ struct Engine {
     // the consumer team finishes in the idle ring (kCapTail entries)
     constexpr int kCap = Tm::kSize == ConsTeam::kSize ? kCapTail : kCapSB;
     if (rc.kind == kKindGridPref) {
+      // c counts every key that passed the threshold, including those its
+      // region (rc.cand_cap entries) had no room for: every branch that
+      // reads the region first checks that all c entries are in it
       const int c = m->st_candn;
-      if (c >= rc.k && c <= kCap) {
+      if (c >= rc.k && c <= kCap && c <= rc.cand_cap) {
         load_entries<Tm>(ent, cand, c);
         Tm::sync();
         uint64_t prefix = 0;
@@ -2073,7 +2087,7 @@ struct Engine {
         uint32_t* cctr = reinterpret_cast<uint32_t*>(&rs->sb_count);
         uint32_t* octr = reinterpret_cast<uint32_t*>(&rs->out_count);
         uint64_t* dst = p.pb_sb + (size_t)i * kCapSB;
-        auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, kCapSB, &p.hdr->status); };
+        auto flc = [&](const WarpBuf& s) { flush_cand(s, cctr, dst, kCapSB); };
         auto flo = [&](const WarpBuf& s) { flush_out<VT>(p, s, octr, rc.out_off, rc.k); };
         const int64_t a = (int64_t)(w - t->c0[i]) * t->chunk, b = min((int64_t)len, a + t->chunk);
         pb_source(rc, src, a, b, [&](uint32_t bits, int64_t pos, bool ok) {
@@ -2366,7 +2380,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   int NA, NB, lag, fin_tail;
   int una = 1, unc = 0, ufin = 0;
   if (p.uniform) {
-    const int kind = row_kind(p.u_n, p.u_k);
+    const int kind = row_kind(p.u_n, p.u_k, p.cta_cap);
     una = row_na(kind, p.u_n, p.CH, p.CHR);
     unc = row_nbc(kind, p.u_n, p.CH, p.CHR);
     ufin = row_fin(kind);
@@ -2468,15 +2482,21 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
 template <int VT, bool SCALE>
 inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t stream) {
   auto kern = dev::engine_kernel<VT, SCALE>;
-  // The smem opt-in is per device; remember which devices have it.
+  // The smem opt-in is per device; remember which devices have it.  Callers
+  // on several host threads (a serving worker beside the application) may
+  // launch at once, so the table is guarded.
+  static std::mutex attr_mu;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  {
+    std::lock_guard<std::mutex> lock(attr_mu);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
   }
   // Cooperative launch: phase B synchronises the grid, so every CTA must be
   // resident (one per SM).

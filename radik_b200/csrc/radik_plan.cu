@@ -40,8 +40,8 @@ __device__ int64_t block_excl_scan64(int64_t v, int64_t* scan, int64_t* total) {
 // end of the block of row r + D, or in a tail after the last block); and
 // the claim-order lag that keeps every B item after its row's A items.
 __global__ void __launch_bounds__(kThreads, 1)
-    plan_kernel(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
-                int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
+    plan_kernel(const RowDesc* desc, int B, int CH, int CHR, int cta_cap, int D, uint32_t flags, RowPlan* plans,
+                int32_t* a_row, int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
                 int64_t sort_cap_total, int grid) {
   __shared__ int64_t scan[32];
   __shared__ int64_t run[5];
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool sorted = (flags & kFlagSorted) != 0;
   auto kind_of = [&](int r) {
     const RowDesc d = desc[r];
-    return row_kind(d.n < 0 ? 0 : d.n, d.k);
+    return row_kind(d.n < 0 ? 0 : d.n, d.k, cta_cap);
   };
   for (int base = 0; base < B; base += kThreads) {
     const int r = base + threadIdx.x;
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (r < B) {
       d = desc[r];
       if (d.n < 0) d.n = 0;
-      kind = row_kind(d.n, d.k);
+      kind = row_kind(d.n, d.k, cta_cap);
       na = row_na(kind, d.n, CH, CHR);
       blk = row_nbc(kind, d.n, CH, CHR) + ((r >= D) ? row_fin(kind_of(r - D)) : 0);
       cand = row_cand_cap(kind, d.n);
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int64_t tail_base = run[1];
   for (int r = warp; r < B; r += kWarps) {
     const RowPlan& pl = plans[r];
-    const int kind = row_kind(pl.n, pl.k);
+    const int kind = row_kind(pl.n, pl.k, cta_cap);
     const int32_t na = row_na(kind, pl.n, CH, CHR), nbc = row_nbc(kind, pl.n, CH, CHR);
     for (int c = lane; c < na; c += 32) a_row[pl.a0 + c] = r;
     for (int c = lane; c < nbc; c += 32) b_row[pl.b0 + c] = r;
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         int64_t pos;
         if (r + D < B) {
           const RowPlan& q = plans[r + D];
-          pos = q.b0 + row_nbc(row_kind(q.n, q.k), q.n, CH, CHR);
+          pos = q.b0 + row_nbc(row_kind(q.n, q.k, cta_cap), q.n, CH, CHR);
         } else {
           int64_t t = 0;  // FIN items of rows B-Dd .. r-1
           for (int x = B - Dd; x < r; ++x) t += row_fin(kind_of(x)) ? 1 : 0;
@@ -170,11 +170,11 @@ cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream
   }
 }
 
-cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int D, uint32_t flags, RowPlan* plans, int32_t* a_row,
-                        int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap, int64_t cand_cap_total,
-                        int64_t sort_cap_total, int grid, cudaStream_t stream) {
-  dev::plan_kernel<<<1, kThreads, 0, stream>>>(desc, B, CH, CHR, D, flags, plans, a_row, b_row, hdr, na_cap, nb_cap,
-                                               cand_cap_total, sort_cap_total, grid);
+cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int cta_cap, int D, uint32_t flags,
+                        RowPlan* plans, int32_t* a_row, int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap,
+                        int64_t cand_cap_total, int64_t sort_cap_total, int grid, cudaStream_t stream) {
+  dev::plan_kernel<<<1, kThreads, 0, stream>>>(desc, B, CH, CHR, cta_cap, D, flags, plans, a_row, b_row, hdr, na_cap,
+                                               nb_cap, cand_cap_total, sort_cap_total, grid);
   return cudaGetLastError();
 }
 

@@ -411,23 +411,28 @@ int radik_server_run_trace(radik_server* h, const radik_trace_item* items, int c
   for (int i = 0; i < count; ++i) {
     const radik_trace_item& it = items[i];
     const double due = t0 + it.arrival_us;
+    // sleep through long gaps, then spin the last stretch for an exact arrival
+    const double early = due - now_us() - 150.0;
+    if (early > 0) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)early));
     while (now_us() < due) {
     }
     const int rc = radik_server_submit(h, it.dtype, it.flags, it.values, it.n, it.k, it.val_out, it.idx_out, &ids[i]);
     if (rc != RADIK_OK) return rc;
   }
   const int rc = radik_server_drain(h);
-  if (latency_us) {
-    std::vector<radik_completion> done;
-    {
-      std::lock_guard<std::mutex> lock(S.mu);
-      done.swap(S.completed);
+  if (latency_us && count > 0) {
+    // Take this trace's completions (ids are consecutive from ids[0], as no
+    // other thread submits meanwhile); completions of requests submitted
+    // before the trace stay queued for radik_server_poll.
+    std::lock_guard<std::mutex> lock(S.mu);
+    size_t w = 0;
+    for (size_t r = 0; r < S.completed.size(); ++r) {
+      const radik_completion& c = S.completed[r];
+      const uint64_t j = c.id - ids[0];
+      if (c.id >= ids[0] && j < (uint64_t)count) latency_us[j] = c.latency_us;
+      else S.completed[w++] = c;
     }
-    // ids are consecutive from ids[0]
-    for (const radik_completion& c : done) {
-      const int64_t j = (int64_t)(c.id - ids[0]);
-      if (count > 0 && j >= 0 && j < count) latency_us[j] = c.latency_us;
-    }
+    S.completed.resize(w);
   }
   return rc;
 }

@@ -49,7 +49,7 @@ def test_workspace_size_monotone():
     assert a <= b <= c
     s = rk.get_radix_select_l_workspace_size(rk.F32, 1 << 16, 1 << 24, 1, rk.SORTED)
     u = rk.get_radix_select_l_workspace_size(rk.F32, 1 << 16, 1 << 24, 1, 0)
-    assert s > u  # sort scratch for k > 16384
+    assert s > u  # merge-sort scratch for k > 4096
 
 
 def _call(dtype=rk.F32, flags=0, ws=1 << 12, val=1 << 12, out=1 << 12, idx_in=None, lens=(10,), K=4):
@@ -90,3 +90,25 @@ def test_autotune_rejects_empty_call_without_device():
     arr = (ctypes.c_int * 1)(0)
     rc = rk.lib().radik_autotune(rk.F32, 0, 1 << 12, None, 1 << 12, 1 << 12, 1 << 12, 1 << 20, arr, 0, 4, None, None)
     assert rc == rk.EINVAL
+
+
+def test_tuning_table_round_trip_without_device(tmp_path):
+    """radik_autotune_load / _save: a table of buckets reloads unchanged; a
+    malformed one is rejected."""
+    good = tmp_path / "t.txt"
+    good.write_text("# comment\n14208 0 0 65536\n24280 65536 11 131072\n")
+    try:
+        rk.autotune_load(str(good))
+        out = tmp_path / "u.txt"
+        rk.autotune_save(str(out))
+        lines = [l for l in out.read_text().splitlines() if not l.startswith("#")]
+        assert lines == ["14208 0 0 65536", "24280 65536 11 131072"]
+        bad = tmp_path / "b.txt"
+        bad.write_text("14208 0 0\n")
+        with pytest.raises(rk.RadikError):
+            rk.autotune_load(str(bad))
+        bad.write_text("14208 1000 0 0\n")  # chunk below the 4096-key minimum
+        with pytest.raises(rk.RadikError):
+            rk.autotune_load(str(bad))
+    finally:
+        rk.autotune_reset()

@@ -268,16 +268,47 @@ def test_topk_rows_replayed_from_cuda_graph():
         assert_same_selection((vals.cpu().numpy(), idx.cpu().numpy()), (ov, oi), ns, ks, oo, True, f"seed {seed}")
 
 
-def test_autotune_keeps_results_exact():
-    n, B, k = 1 << 20, 32, 256
+@pytest.mark.parametrize("shape", [(32, 1 << 20, 256), (2, 1 << 20, 20000), (16, 200000, 300)],
+                         ids=["pref", "radix", "cta-cap"])
+def test_autotune_keeps_results_exact(shape, tmp_path):
+    """Whatever the tuner picks (chunk, first digit, CTA row cap), results
+    stay bit-identical, and a saved table reloads to the same choice."""
+    B, n, k = shape
     flat = np.concatenate([values_for(rk.F32, n, "normal", 900 + r) for r in range(B)])
     t = to_dev(flat, rk.F32).view(B, n)
     before = rk.topk(t, k, largest=True, sorted=True)
     try:
-        ch = rk.autotune(t, k, largest=True, sorted=True)
-        assert ch >= 4096 and (ch & (ch - 1)) == 0
+        c = rk.autotune(t, k, largest=True, sorted=True)
+        assert c["ms"] > 0
+        assert c["chunk"] == 0 or (c["chunk"] >= 4096 and (c["chunk"] & (c["chunk"] - 1)) == 0)
         after = rk.topk(t, k, largest=True, sorted=True)
         assert torch.equal(before[0], after[0]) and torch.equal(before[1], after[1])
+        path = str(tmp_path / "tune.txt")
+        rk.autotune_save(path)
+        rk.autotune_reset()
+        rk.autotune_load(path)
+        again = rk.topk(t, k, largest=True, sorted=True)
+        assert torch.equal(before[0], again[0]) and torch.equal(before[1], again[1])
+    finally:
+        rk.autotune_reset()
+
+
+def test_autotune_rows_keeps_results_exact():
+    ns, ks = workloads.uneven_rows(96, 5, 10, 20, 2048)
+    flat = np.concatenate([values_for(rk.F32, m, "normal", 70 + r) for r, m in enumerate(ns)])
+    offs = np.concatenate([[0], np.cumsum(ns)[:-1]])
+    oo = np.concatenate([[0], np.cumsum(ks)[:-1]])
+    rows = [(int(a), int(b), int(n), int(k)) for a, b, n, k in zip(offs, oo, ns, ks)]
+    x = to_dev(flat, rk.F32)
+    host = (rk.RowDesc * len(rows))(*[rk.RowDesc(*r) for r in rows])
+    desc = torch.frombuffer(bytearray(bytes(host)), dtype=torch.uint8).to(DEV)
+    bounds = (sum(ns), max(ns), max(ks))
+    try:
+        c = rk.autotune_rows(x, desc, len(rows), bounds, int(sum(ks)), largest=True)
+        assert c["ms"] > 0
+        gv, gi = rk.topk_rows(x, rows, largest=True)
+        ov, oi = oracle.topk(flat, ns, ks, flags=oracle.flags_of(True, False), out_offsets=oo)
+        assert_same_selection((gv.cpu().numpy(), gi.cpu().numpy()), (ov, oi), ns, ks, oo, False)
     finally:
         rk.autotune_reset()
 
@@ -292,3 +323,28 @@ def test_single_huge_row(dist, k):
     for largest in (True, False):
         got, want = run_both(flat, [n], k, rk.F32, largest, True)
         assert_same_selection(got, want, [n], [k], [0], True, f"{dist} largest={largest}")
+
+
+def test_uneven_lengths_refuse_stream_capture():
+    """radik_topk copies the descriptors of unequal rows from host memory that
+    lives only for the call, so a capture of it is refused (RADIK_ENOTSUP);
+    radik_topk_rows, with device descriptors, is the capturable form."""
+    lengths = [5000, 70000, 300]
+    x = to_dev(values_for(rk.F32, sum(lengths), "normal", 1), rk.F32)
+    rk.topk(x, 10, lengths)  # outside a capture: fine
+    graph = torch.cuda.CUDAGraph()
+    with pytest.raises(rk.RadikError) as err:
+        with torch.cuda.graph(graph):
+            rk.topk(x, 10, lengths, check=False)
+    assert err.value.code == rk.ENOTSUP
+
+
+@pytest.mark.parametrize("dist", ["zero", "mantissa_noise", "constant_heavy", "ties"])
+def test_several_rows_in_phase_b(dist):
+    """Several rows of one batch whose sampled threshold catches too many keys
+    (ties) finish together in the grid-wide phase B."""
+    n, B = 1 << 21, 3
+    flat = np.concatenate([values_for(rk.F32, n, dist, 50 + r) for r in range(B)])
+    for largest, k in ((True, 100), (False, 3000), (True, 20000)):
+        got, want = run_both(flat, [n] * B, k, rk.F32, largest, True)
+        assert_same_selection(got, want, [n] * B, [k] * B, [r * k for r in range(B)], True, f"{dist} k={k}")

@@ -1,10 +1,14 @@
 """Serving loop (radik_server_*): a request's result is the same alone, in a
 mixed batch stream, in the per-request baseline mode, and from radik_topk --
-bit-exact, since the selection is exact and ties go to the lowest positions."""
+bit-exact, since the selection is exact and ties go to the lowest positions --
+and every request of the mix equals the CPU oracle on its own row."""
 import numpy as np
 import pytest
 
+import oracle
 from radik_b200 import workloads
+
+from conftest import assert_same_selection
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -50,11 +54,13 @@ def test_result_same_alone_and_in_the_mix(sorted_):
     for a, b in ((alone, (pv, pi)), (alone, (ref_v.view(-1), ref_i.view(-1)))):
         ka, kb = key(*a), key(*b)
         assert torch.equal(ka[0], kb[0]) and torch.equal(ka[1], kb[1])
-    # every request of the mix against radik_topk on its own
-    for x, v, i in mix[::7]:
-        rv, ri = rk.topk(x, v.numel(), sorted=sorted_)
-        ka, kb = key(v, i), key(rv.view(-1), ri.view(-1))
-        assert torch.equal(ka[0], kb[0]) and torch.equal(ka[1], kb[1])
+    # every request of the mix against the oracle on its own row
+    for j, (x, v, i) in enumerate(mix):
+        xh = x.cpu().numpy()
+        k = v.numel()
+        want = oracle.topk(xh, [xh.size], k, flags=oracle.flags_of(True, sorted_))
+        assert_same_selection((v.cpu().numpy(), i.cpu().numpy()), want, [xh.size], [k], [0], sorted_,
+                              f"request {j} (n={xh.size}, k={k}, {x.dtype})")
 
 
 def test_per_request_mode_and_small_budget():

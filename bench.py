@@ -403,30 +403,51 @@ def run_skew(impl, args, dev, stream, peak, peak_kind):
             def step():
                 impl.call(x, vals, idx, ws, [n], k, True, False)
 
+            def exact():
+                gv = _bits(vals[:k].cpu().numpy())
+                gi = idx[:k].cpu().numpy().astype(np.int64)
+                if impl.name == "reference":
+                    return bool(np.array_equal(np.sort(gv), np.sort(ov[:k])))
+                o = np.argsort(gi, kind="stable")
+                w = np.argsort(oi[:k], kind="stable")
+                return bool(np.array_equal(gi[o], oi[:k][w]) and np.array_equal(gv[o], ov[:k][w]))
+
             for _ in range(args.warmup):
                 step()
             _, ts = time_steps(step, reps, stream, lambda: flush_buf.zero_())
             impl.check_status(ws)
             ms = statistics.median(ts)
-            gv = _bits(vals[:k].cpu().numpy())
-            gi = idx[:k].cpu().numpy().astype(np.int64)
-            if impl.name == "reference":
-                ok = bool(np.array_equal(np.sort(gv), np.sort(ov[:k])))
-            else:
-                o = np.argsort(gi, kind="stable")
-                w = np.argsort(oi[:k], kind="stable")
-                ok = bool(np.array_equal(gi[o], oi[:k][w]) and np.array_equal(gv[o], ov[:k][w]))
-            if not ok:
+            if not exact():
                 bad_cases.append(f"{dname}/k={k}")
-            sweep.append({"dist": dname, "k": k, "ms": round(ms, 4), "gkeys": round(n / (ms / 1e3) / 1e9, 2),
-                          "frac": round((n * 4 + k * 8) / (ms / 1e3) / 1e9 / peak, 4)})
+            case = {"dist": dname, "k": k, "ms": round(ms, 4), "gkeys": round(n / (ms / 1e3) / 1e9, 2),
+                    "frac": round((n * 4 + k * 8) / (ms / 1e3) / 1e9 / peak, 4)}
+            if impl.name == "radik_b200" and not args.no_tune:
+                # the autotuner on this case's shape bucket, then the same timing
+                choice = impl.rk.autotune(x.view(1, n), k, largest=True, sorted=False, workspace=ws, stream=stream)
+                for _ in range(2):
+                    step()
+                _, ts = time_steps(step, reps, stream, lambda: flush_buf.zero_())
+                impl.check_status(ws)
+                tms = statistics.median(ts)
+                if not exact():
+                    bad_cases.append(f"{dname}/k={k} tuned")
+                case.update({"tuned_ms": round(tms, 4), "tuned_gkeys": round(n / (tms / 1e3) / 1e9, 2),
+                             "tuned": {c: v for c, v in choice.items() if c != "ms"}})
+            sweep.append(case)
+    if impl.name == "radik_b200" and not args.no_tune:
+        impl.rk.autotune_reset()
     g = float(np.exp(np.mean([np.log(c["gkeys"]) for c in sweep])))
     worst = min(sweep, key=lambda c: c["gkeys"])
     fr = float(np.exp(np.mean([np.log(c["frac"]) for c in sweep])))
+    tuned = None
+    if sweep and "tuned_gkeys" in sweep[0]:
+        tg = float(np.exp(np.mean([np.log(c["tuned_gkeys"]) for c in sweep])))
+        tuned = {"geomean_gkeys_per_s": round(tg, 2), "speedup_vs_default": round(tg / g, 3),
+                 "note": "radik_autotune per case (chunk length, first digit, one-CTA row cap), then re-timed"}
     return {"workload": "skew sweep, single fp32 rows n = 2^24, k = 2^4..2^16, U(0,1) / 1.0f + low-8-bit mantissa "
                         "noise / Zipf(1.1) ranks / 90% constant 0.5 + 10% U(0,1); largest, unsorted",
             "cases": len(sweep), "geomean_gkeys_per_s": round(g, 2), "geomean_frac": round(fr, 4),
-            "worst": worst, "l2": "flushed (256 MiB write) before every timed launch", "reps": reps,
+            "worst": worst, "tuned": tuned, "l2": "flushed (256 MiB write) before every timed launch", "reps": reps,
             "parity": {"cases": len(sweep), "exact": not bad_cases, "mismatched": bad_cases,
                        "checked": ("value multisets" if impl.name == "reference" else
                                    "values bit-exact and index sets") + " vs oracle"},
@@ -557,11 +578,41 @@ def run_uneven(impl, args, dev, stream, peak, peak_kind):
     span_pr, _ = time_steps(per_row, 2, stream)
     per_row_ms = span_pr / 2
     rk.status(ws_row, stream)
+    tuned = None
+    if not args.no_tune:
+        # the autotuner on the rows form (chunk length, first digit, one-CTA
+        # row cap), then a graph captured with the chosen configuration
+        choice = rk.autotune_rows(dev_in, desc_dev, B, (total_n, n_max, k_max), total_out, largest=True,
+                                  workspace=ws, stream=stream)
+        for _ in range(2):
+            call()
+        torch.cuda.synchronize(dev)
+        graph_t = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph_t):
+            call()
+        torch.cuda.synchronize(dev)
+        for _ in range(2):
+            graph_t.replay()
+        span_t, _ = time_steps(graph_t.replay, args.steps, stream)
+        rk.status(ws, stream)
+        tms = span_t / args.steps
+        gvt, git = _bits(vals.cpu().numpy()), idx.cpu().numpy().astype(np.int64)
+        bad_t = 0
+        for r in range(B):
+            a, b = int(oo[r]), int(oo[r] + ks[r])
+            o = np.argsort(git[a:b], kind="stable")
+            if not (np.array_equal(git[a:b][o], oi[a:b]) and np.array_equal(gvt[a:b][o], ov[a:b])):
+                bad_t += 1
+        bad += bad_t
+        rk.autotune_reset()
+        tuned = {"one_launch_ms": round(tms, 4), "gkeys_per_s": round(total_n / (tms / 1e3) / 1e9, 3),
+                 "speedup_vs_default": round(ms / tms, 3), "speedup_vs_per_row": round(per_row_ms / tms, 2),
+                 "choice": {c: v for c, v in choice.items() if c != "ms"}, "mismatched_rows": bad_t}
     res.update({"one_launch_ms": round(ms, 4), "gkeys_per_s": round(total_n / (ms / 1e3) / 1e9, 3),
                 "per_row_ms": round(per_row_ms, 3),
                 "per_row_gkeys_per_s": round(total_n / (per_row_ms / 1e3) / 1e9, 3),
                 "speedup_vs_per_row": round(per_row_ms / ms, 2), "cuda_graph": True, "steps": args.steps,
-                "launches_per_step": 2})
+                "launches_per_step": 2, "tuned": tuned})
     res["roofline"] = roofline(algo_bytes, statistics.mean(step_ms), peak, peak_kind)
     res["parity"] = {"rows": B, "exact": bad == 0, "mismatched_rows": bad,
                      "checked": "one-launch form: values bit-exact and index sets vs oracle"}
@@ -712,6 +763,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the output checks (profiling runs)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuned re-timings (skew, uneven)")
     ap.add_argument("--rows", type=int, default=0, help="override the row count (profiling a smaller case)")
     ap.add_argument("--serving-requests", type=int, default=10000)
     args = ap.parse_args()

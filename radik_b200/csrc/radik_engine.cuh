@@ -651,14 +651,24 @@ __device__ __forceinline__ void flush_cand(const WarpBuf& s, uint32_t* ctr, uint
 // ----------------------------------------------------------------------------
 // Shared-memory selection
 // ----------------------------------------------------------------------------
+// Warp-wide min / max of 64-bit values with the 32-bit redux unit: the high
+// words first, then the low words of the lanes holding that high word.
+__device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
+  const uint32_t h = __reduce_min_sync(kFull, (uint32_t)(v >> 32));
+  const uint32_t l = __reduce_min_sync(kFull, (uint32_t)(v >> 32) == h ? (uint32_t)v : 0xFFFFFFFFu);
+  return ((uint64_t)h << 32) | l;
+}
+__device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
+  const uint32_t h = __reduce_max_sync(kFull, (uint32_t)(v >> 32));
+  const uint32_t l = __reduce_max_sync(kFull, (uint32_t)(v >> 32) == h ? (uint32_t)v : 0u);
+  return ((uint64_t)h << 32) | l;
+}
+
 // Block-wide min of lo and max of hi over all threads (pass ~0 / 0 to abstain).
 template <class Tm>
 __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t* mn, uint64_t* mx, Misc* m) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)lo, o));
-    hi = max(hi, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)hi, o));
-  }
+  lo = warp_min64(lo);
+  hi = warp_max64(hi);
   uint64_t* red = reinterpret_cast<uint64_t*>(m->scan);  // 64 x u32 = 32 x u64
   const int warp = Tm::wid(), lane = threadIdx.x & 31;
   Tm::sync();
@@ -669,11 +679,8 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
   Tm::sync();
   if (warp == 0) {
     uint64_t a = lane < Tm::kWarps ? red[lane] : ~0ull, b = lane < Tm::kWarps ? m->red_hi_w[lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a = min(a, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)a, o));
-      b = max(b, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)b, o));
-    }
+    a = warp_min64(a);
+    b = warp_max64(b);
     if (lane == 0) {
       m->red_lo = a;
       m->red_hi = b;
@@ -691,39 +698,46 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
 // When bits remain after that, the upper edge of the r-th key's bin is
 // returned (at least r keys are <= it).  hist: 4096 counters of smem.
 // Finds the bin b of h[0..256) with cum(<b) < krem <= cum(<=b) using one
-// warp (8 bins a lane, then a warp scan).  Result in m->sel_*; m->sel_found
-// = 0 if the bins hold fewer than krem.  Ends with a team barrier.
+// warp.  Lane l reads bins l, l + 32, ..., l + 224 (no bank conflicts), the
+// eight columns are scanned across the lanes side by side, and a ballot per
+// column finds the first bin whose running count reaches krem.  Result in
+// m->sel_*; m->sel_found = 0 if the bins hold fewer than krem (or krem is
+// 0).  Ends with a team barrier.
 template <class Tm>
 __device__ void select256(const uint32_t* hist, uint32_t krem, Misc* m) {
   if (Tm::wid() == 0) {
     const int lane = threadIdx.x & 31;
-    uint32_t c[8], s = 0;
+    uint32_t c[8], incl[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      c[j] = hist[lane * 8 + j];
-      s += c[j];
+      c[j] = hist[j * 32 + lane];
+      incl[j] = c[j];
     }
-    uint32_t incl = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    if (lane == 0 && total < krem) m->sel_found = 0;
-    uint32_t run = incl - s;
-    if (run < krem && krem <= incl) {
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        if (run + c[j] >= krem && run < krem) {
-          m->sel_bin = (uint32_t)(lane * 8 + j);
-          m->sel_cum = run;
+        const uint32_t y = __shfl_up_sync(kFull, incl[j], o);
+        if (lane >= o) incl[j] += y;
+      }
+    }
+    uint32_t base = 0;
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const unsigned hit = __ballot_sync(kFull, krem > 0 && base + incl[j] >= krem);
+      if (!found && hit) {
+        found = true;
+        if (lane == __ffs(hit) - 1) {
+          m->sel_bin = (uint32_t)(j * 32 + lane);
+          m->sel_cum = base + incl[j] - c[j];
           m->sel_cnt = c[j];
           m->sel_found = 1;
         }
-        run += c[j];
       }
+      base += __shfl_sync(kFull, incl[j], 31);
     }
+    if (!found && lane == 0) m->sel_found = 0;
   }
   Tm::sync();
 }
@@ -737,8 +751,16 @@ __device__ void select256(const uint32_t* hist, uint32_t krem, Misc* m) {
 template <class Tm, int KB>
 __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r, uint64_t lo, uint64_t hi,
                                            uint32_t* hist, Misc* m, int32_t* status) {
+  // Small ranks (r <= a quarter of the team) select among the per-thread
+  // minimums instead of all cnt keys: the r-th smallest minimum has r
+  // distinct sampled keys at or below it, so it bounds the r-th smallest key
+  // from above, and for r << team size it sits at nearly the same quantile
+  // (the minimum of m keys is below x with probability about m times that of
+  // one key).  Each level then counts one value a thread instead of cnt /
+  // team: the shared-memory atomics were most of a level's time.
+  const bool by_mins = r * 4 <= Tm::kSize;
   uint64_t mn, mx;
-  block_minmax<Tm>(lo, hi, &mn, &mx, m);
+  block_minmax<Tm>(lo, by_mins ? (lo == ~0ull ? 0ull : lo) : hi, &mn, &mx, m);
   if (mn >= mx) return (uint32_t)mn;
   int plen = __clzll((long long)(mn ^ mx)) - (64 - KB);  // shared leading bits
   uint32_t prefix = plen > 0 ? (uint32_t)(mn >> (KB - plen)) : 0u;
@@ -749,17 +771,23 @@ __device__ uint32_t block_sample_threshold(const uint32_t* keys, int cnt, int r,
     for (int i = Tm::tid(); i < 256; i += Tm::kSize) hist[i] = 0;
     Tm::sync();
     const int sd = KB - plen - D;
-    for (int b = 0; b < cnt; b += 4 * Tm::kSize) {  // four keys a thread in flight
-      uint32_t k[4];
+    if (by_mins) {
+      const uint32_t v = (uint32_t)lo;
+      if (lo != ~0ull && (plen == 0 || (v >> (KB - plen)) == prefix)) atomicAdd(&hist[(v >> sd) & (uint32_t)(NB - 1)], 1u);
+    } else {
+      for (int b = 0; b < cnt; b += 4 * Tm::kSize) {  // four keys a thread in flight
+        uint32_t k[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = b + u * Tm::kSize + Tm::tid();
-        k[u] = i < cnt ? keys[i] : 0u;
-      }
+        for (int u = 0; u < 4; ++u) {
+          const int i = b + u * Tm::kSize + Tm::tid();
+          k[u] = i < cnt ? keys[i] : 0u;
+        }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = b + u * Tm::kSize + Tm::tid();
-        if (i < cnt && (plen == 0 || (k[u] >> (KB - plen)) == prefix)) atomicAdd(&hist[(k[u] >> sd) & (uint32_t)(NB - 1)], 1u);
+        for (int u = 0; u < 4; ++u) {
+          const int i = b + u * Tm::kSize + Tm::tid();
+          if (i < cnt && (plen == 0 || (k[u] >> (KB - plen)) == prefix))
+            atomicAdd(&hist[(k[u] >> sd) & (uint32_t)(NB - 1)], 1u);
+        }
       }
     }
     Tm::sync();
@@ -869,10 +897,12 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
 }
 
 // Emits the entries selected by (prefix, plen) to the row's output, in entry
-// order, reserving the slots with one atomic on the row's out_count.
+// order, reserving the slots with one atomic on the row's out_count -- or,
+// when the team is the row's only writer (sole), from slot 0 without it: the
+// atomic's round trip sits on the finish's critical path.
 template <class Tm, int VT, bool SCALE, typename G>
 __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& rc, uint64_t prefix, int plen,
-                          RowState* rs, Misc* m) {
+                          RowState* rs, Misc* m, bool sole = false) {
   using K = KT<VT, SCALE>;
   const int W = K::KB + rc.IB;
   const int sh = W - plen;
@@ -889,9 +919,13 @@ __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& r
   }
   uint32_t total;
   const uint32_t ex = block_excl_scan<Tm>(mine, m->scan, &total);
-  if (Tm::tid() == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
-  Tm::sync();
-  int64_t slot = (int64_t)m->counter + ex;
+  uint32_t base = 0;
+  if (!sole) {
+    if (Tm::tid() == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
+    Tm::sync();
+    base = m->counter;
+  }
+  int64_t slot = (int64_t)base + ex;
   for (int i = lo; i < hi; ++i) {
     uint32_t bits;
     int64_t pos;
@@ -1260,7 +1294,7 @@ struct Engine {
     };
     smem_resolve<SideTeam, VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
                             &p.hdr->status);
-    smem_emit<SideTeam, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m);
+    smem_emit<SideTeam, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m, true);
     post_process<SideTeam, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
   }
 
@@ -1324,7 +1358,7 @@ struct Engine {
         int plen = 0, krem = rc.k;
         smem_resolve<SideTeam, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                                 &p.hdr->status);
-        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m, true);
         post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
         return;
       }
@@ -1851,7 +1885,8 @@ struct Engine {
         int plen = 0, krem = rc.k;
         smem_resolve<Tm, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kCap * 8), m,
                                 &p.hdr->status);
-        smem_emit<Tm, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m);
+        // a pre-filter row's outputs are written by its finish alone
+        smem_emit<Tm, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m, true);
         post_process<Tm, VT, SCALE>(p, rc, smem, m);
       } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax) && p.B >= kSideResolveMinRows) {
         side_cand_resolve<Tm>(r, rc, c, 0, 0, rc.k, c);

@@ -71,10 +71,15 @@ BATCHED = {
 VARIANTS = ("batched_k32", "batched_k1024", "batched_f16", "batched_sorted", "batched_smallest")
 
 # DRAM bytes (read + write) per engine launch measured by ncu, keyed by
-# workload and rows, with the hash of the engine sources they were captured
-# from (engine_source_hash()).  A figure whose hash differs from the sources
-# being run describes an older kernel and is not reported.
-NCU_TRAFFIC = {}
+# workload and rows: (hash of the engine sources captured, bytes, how).  A
+# figure whose hash differs from the sources being run describes an older
+# kernel and is not reported.
+NCU_TRAFFIC = {
+    ("batched", 256): ("7e3ae98bb522059e", 1094895734,
+                       "mean of 13 full-size launches"),
+    ("batched_f16", 256): ("7e3ae98bb522059e", 4 * 139484672,
+                           "64-row capture x 4 (traffic grows with the rows streamed)"),
+}
 
 
 def engine_source_hash() -> str:
@@ -91,10 +96,10 @@ def traffic_of(workload, rows):
     t = NCU_TRAFFIC.get((workload, rows))
     if t is None:
         return None, "no ncu capture of this workload"
-    src, bytes_ = t
+    src, bytes_, how = t
     if src != engine_source_hash():
         return None, f"ncu capture from engine sources {src}; current sources differ"
-    return bytes_, f"ncu dram__bytes_read.sum + dram__bytes_write.sum, engine sources {src}"
+    return bytes_, f"ncu dram__bytes_read.sum + dram__bytes_write.sum, engine sources {src}, {how}"
 
 
 def load_peaks():
@@ -176,6 +181,11 @@ def time_steps(step, steps, stream, flush=None):
 
     evs = [(_event(), _event()) for _ in range(steps)]
     t0, t1 = _event(), _event()
+    # A device-side delay ahead of the span lets the host enqueue the steps
+    # before the GPU reaches them, so the span holds the GPU's time for the
+    # K steps and not the host's time to issue the first of them.
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(min(200_000 * steps, 100_000_000))
     t0.record(stream)
     for i in range(steps):
         if flush is not None:

@@ -146,6 +146,7 @@ int env_int(const char* name, int dflt) {
 // RADIK_CHR / RADIK_D1 / RADIK_CTA_CAP override everything (tuning sweeps).
 struct Config {
   int CH, CHR, D1, cta_cap;
+  int early_copy;  // chunk copies may start before their row's threshold exists
 };
 
 // A tuned shape bucket: a field of 0 keeps the built-in choice.
@@ -184,13 +185,20 @@ Tuned tuned_for(uint64_t bucket) {
   return it == g_tuned.end() ? Tuned{} : it->second;
 }
 
-int cta_cap_of(const Tuned& t) {
+// Rows of up to this many keys are selected by one CTA.  A call of few rows
+// (fewer than half the CTAs) leaves most of the grid idle that way, so there
+// only rows of up to 2^15 keys stay on one CTA and longer ones spread over
+// the grid (one 100K-key row: 97 us on one CTA's side team).
+int cta_cap_of(const Tuned& t, int B, int grid) {
   const int ecap = env_int("RADIK_CTA_CAP", 0);
   if (ecap >= kCtaRowCapMin && ecap <= kCtaRowCapMax) return ecap;
-  return t.cta_cap ? t.cta_cap : kCtaRowCap;
+  if (t.cta_cap) return t.cta_cap;
+  return B * 2 < grid ? kCtaRowCapMin : kCtaRowCap;
 }
 
-Config choose_config(int64_t stream_elems, int grid, const Tuned& t) {
+// stream_elems: keys of the call's streamed rows; es: bytes per key; uniform_n:
+// the common row length of an equal-length call (0 otherwise) and B its rows.
+Config choose_config(int64_t stream_elems, int grid, const Tuned& t, int es, int uniform_n, int B = 0) {
   Config c{};
   const int64_t target = std::max<int64_t>(1, stream_elems / ((int64_t)grid * 8));
   int ch = kMinCH;
@@ -199,16 +207,37 @@ Config choose_config(int64_t stream_elems, int grid, const Tuned& t) {
   // balance, so no chunk is shorter than 128K keys (single 2^24-key rows:
   // 154 -> 111 us from 8K to 128K chunks).
   if (stream_elems >= ((int64_t)1 << 24)) ch = std::max(ch, 1 << 17);
+  // A chunk item costs about 2 us of turnover whatever its length, so 16-bit
+  // keys take chunks of the same bytes, not the same keys (fp16 256 x 2^20:
+  // 175.7 -> 165.3 us from 128K to 256K keys).
+  if (es == 2 && ch >= (1 << 17)) ch = std::min(kMaxCH, ch * 2);
+  // Small equal-length calls: one chunk per CTA at most, so no CTA claims a
+  // second item (single 2^20-key rows took 256 chunks of 4K keys over 148
+  // CTAs before).  Each row splits into as many chunks as the grid has CTAs
+  // per row, rounded down; a few rows leave their sampling CTAs out.
+  const int spread = std::max(1, grid - (B > 0 && B * 2 < grid ? B : 0));
+  const int64_t per_cta = (stream_elems + spread - 1) / spread;
+  if (uniform_n > 0 && per_cta <= kMaxCH) {
+    const int64_t cpr = std::max<int64_t>(1, uniform_n / std::max<int64_t>(1, per_cta));
+    int64_t len = (uniform_n + cpr - 1) / cpr;
+    len = (len + 31) / 32 * 32;
+    ch = (int)std::min<int64_t>(kMaxCH, std::max<int64_t>(kMinCH, len));
+  }
   c.CH = t.ch ? t.ch : ch;
   c.CHR = 32768;
   c.D1 = t.d1 ? t.d1 : kMaxD1;
-  c.cta_cap = cta_cap_of(t);
+  c.cta_cap = cta_cap_of(t, B, grid);
   const int ech = env_int("RADIK_CH", 0);
   if (ech >= kMinCH && ech <= (1 << 24) && (ech % 16) == 0) c.CH = ech;
   const int echr = env_int("RADIK_CHR", 0);
   if (echr >= kMinCH && echr <= (1 << 24) && (echr % 16) == 0) c.CHR = echr;
   const int ed1 = env_int("RADIK_D1", 0);
   if (ed1 >= kMinD1 && ed1 <= kMaxD1) c.D1 = ed1;
+  // Calls that stream at most 64 MiB copy their chunks while the thresholds
+  // are computed: their ring fills cannot delay the sample reads by much.
+  c.early_copy = stream_elems * es <= ((int64_t)64 << 20) ? 1 : 0;
+  const int eec = env_int("RADIK_EARLY", -1);
+  if (eec == 0 || eec == 1) c.early_copy = eec;
   return c;
 }
 
@@ -246,6 +275,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.CHR = c.CHR;
   p.D1 = c.D1;
   p.cta_cap = c.cta_cap;
+  p.early_copy = c.early_copy;
   p.S = kSlots;
   p.flags = flags;
   p.spin_limit = kSpinLimit;
@@ -298,16 +328,16 @@ int plan_call(int dtype, uint32_t flags, const int* task_len, int task_num, int 
   }
   if ((int64_t)B * K > ((int64_t)1 << 40)) return fail(RADIK_EINVAL, "radik: output too large");
   const Tuned t = tuned_for(shape_bucket(dtype, flags, false, B, n_max, K));
-  const int cta_cap = cta_cap_of(t);
+  int grid = 0;
+  int rc = engine_grid(dtype, flags, &grid);
+  if (rc) return rc;
+  const int cta_cap = cta_cap_of(t, B, grid);
   int64_t multi_elems = 0;
   for (int i = 0; i < B; ++i) {
     const int kind = row_kind(task_len[i], K, cta_cap);
     if (kind == kKindAll || kind == kKindGridPref || kind == kKindGridRadix) multi_elems += task_len[i];
   }
-  int grid = 0;
-  int rc = engine_grid(dtype, flags, &grid);
-  if (rc) return rc;
-  const Config cfg = choose_config(multi_elems, grid, t);
+  const Config cfg = choose_config(multi_elems, grid, t, (int)elem_bytes(dtype), uniform ? n_max : 0, B);
   int64_t na = 0, nb = 0, cand = 0, sortn = 0;
   bool has_radix = false;
   for (int i = 0; i < B; ++i) {
@@ -462,7 +492,7 @@ int tune_bucket(uint64_t bucket, cudaStream_t stream, bool has_radix, bool cap_m
     const Tuned base = best;
     for (int ch = std::max(kMinCH, ch_default / 4); ch <= std::min(kMaxCH, ch_default * 4); ch *= 2) {
       Tuned t = base;
-      t.ch = ch;
+      t.ch = (ch + 31) / 32 * 32;  // whole 128-byte lines of 32-bit keys
       trial(t);
     }
   }
@@ -619,7 +649,8 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  const Config cfg = choose_config(total_n, grid, tuned_for(shape_bucket(dtype, flags, true, B, n_max, k_max)));
+  const Config cfg = choose_config(total_n, grid, tuned_for(shape_bucket(dtype, flags, true, B, n_max, k_max)),
+                                   (int)elem_bytes(dtype), 0, B);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(ws, 0, zero_bytes(L, true), stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -676,7 +707,9 @@ int radik_autotune_ex(int dtype, uint32_t flags, const void* val_in, const void*
                 row_kind(n, K, kCtaRowCapMin) == kKindGridRadix;
     cap_matters = cap_matters || (n > kCtaRowCapMin && n <= kCtaRowCapMax && K < n);
   }
-  const Config dflt = choose_config(total, grid, Tuned{});
+  bool uniform = true;
+  for (int i = 0; i < task_num; ++i) uniform = uniform && task_len[i] == task_len[0];
+  const Config dflt = choose_config(total, grid, Tuned{}, (int)elem_bytes(dtype), uniform ? n_max : 0, task_num);
   rc = tune_bucket(bucket, static_cast<cudaStream_t>(stream_), has_radix, cap_matters, dflt.CH,
                    [&] {
                      return radik_topk(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes,
@@ -706,7 +739,7 @@ int radik_autotune_rows(int dtype, uint32_t flags, const void* val_in, const voi
   if (rc) return rc;
   const uint64_t bucket = shape_bucket(dtype, flags, true, task_num, n_max, k_max);
   // the rows live on the device: every knob is tried
-  const Config dflt = choose_config(total_n, grid, Tuned{});
+  const Config dflt = choose_config(total_n, grid, Tuned{}, (int)elem_bytes(dtype), 0, task_num);
   rc = tune_bucket(bucket, static_cast<cudaStream_t>(stream_), true, n_max > kCtaRowCapMin, dflt.CH,
                    [&] {
                      return radik_topk_rows(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes,

@@ -170,6 +170,7 @@ struct EngineParams {
   int32_t CHR;              // chunk length of radix rows (elements), multiple of 16
   int32_t D1;               // first digit width of histogram rows
   int32_t cta_cap;          // rows of up to this many keys are selected by one CTA
+  int32_t early_copy;       // chunk copies may start before their row's threshold exists
   int32_t S;                // hist ring slots
   int32_t lag;              // uniform mode: A-ahead-of-B distance
   int32_t fin_delay;        // uniform mode: rows a FIN item trails its row

@@ -74,6 +74,11 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
   asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
 __device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
   asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -290,7 +295,6 @@ struct Ctrl {
   ItemDesc cq[kQ], sq[kQ];
   uint32_t side_done;       // side items finished (written by the side team)
   uint32_t cons_done;       // consumer items finished (written by the consumer team)
-  int32_t first_q;          // the CTA's first claim
 };
 static_assert(kCtrlOff + 2 * 3072 + sizeof(Ctrl) <= kSmemBytes, "control area");
 
@@ -698,46 +702,48 @@ __device__ __forceinline__ void block_minmax(uint64_t lo, uint64_t hi, uint64_t*
 // When bits remain after that, the upper edge of the r-th key's bin is
 // returned (at least r keys are <= it).  hist: 4096 counters of smem.
 // Finds the bin b of h[0..256) with cum(<b) < krem <= cum(<=b) using one
-// warp.  Lane l reads bins l, l + 32, ..., l + 224 (no bank conflicts), the
-// eight columns are scanned across the lanes side by side, and a ballot per
-// column finds the first bin whose running count reaches krem.  Result in
-// m->sel_*; m->sel_found = 0 if the bins hold fewer than krem (or krem is
-// 0).  Ends with a team barrier.
+// warp.  Lane l holds bins 8l .. 8l + 7 (two 16-byte loads; h is 16-byte
+// aligned), the lanes scan their sums, and the lane whose range reaches krem
+// walks its eight bins.  Few live registers: inside the finishes, where the
+// kernel's register budget is tight, a wider form spilled and took ~8 us.
+// Result in m->sel_*; m->sel_found = 0 if the bins hold fewer than krem (or
+// krem is 0).  Ends with a team barrier.
 template <class Tm>
 __device__ void select256(const uint32_t* hist, uint32_t krem, Misc* m) {
   if (Tm::wid() == 0) {
     const int lane = threadIdx.x & 31;
-    uint32_t c[8], incl[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      c[j] = hist[j * 32 + lane];
-      incl[j] = c[j];
-    }
+    const uint4 a = reinterpret_cast<const uint4*>(hist)[lane * 2];
+    const uint4 b = reinterpret_cast<const uint4*>(hist)[lane * 2 + 1];
+    const uint32_t sum = a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+    uint32_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const uint32_t y = __shfl_up_sync(kFull, incl[j], o);
-        if (lane >= o) incl[j] += y;
-      }
+      const uint32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
     }
-    uint32_t base = 0;
-    bool found = false;
+    const unsigned hit = __ballot_sync(kFull, krem > 0 && incl >= krem);
+    if (hit == 0) {
+      if (lane == 0) m->sel_found = 0;
+    } else if (lane == __ffs(hit) - 1) {
+      uint32_t cum = incl - sum, cnt = 0;
+      int bin = -1;
+      const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const unsigned hit = __ballot_sync(kFull, krem > 0 && base + incl[j] >= krem);
-      if (!found && hit) {
-        found = true;
-        if (lane == __ffs(hit) - 1) {
-          m->sel_bin = (uint32_t)(j * 32 + lane);
-          m->sel_cum = base + incl[j] - c[j];
-          m->sel_cnt = c[j];
-          m->sel_found = 1;
+      for (int t = 0; t < 8; ++t) {
+        if (bin < 0) {
+          if (cum + v[t] >= krem) {
+            bin = t;
+            cnt = v[t];
+          } else {
+            cum += v[t];
+          }
         }
       }
-      base += __shfl_sync(kFull, incl[j], 31);
+      m->sel_bin = (uint32_t)(lane * 8 + bin);
+      m->sel_cum = cum;
+      m->sel_cnt = cnt;
+      m->sel_found = 1;
     }
-    if (!found && lane == 0) m->sel_found = 0;
   }
   Tm::sync();
 }
@@ -899,42 +905,47 @@ __device__ void smem_resolve(G get, int cnt, const RowCtx& rc, uint64_t& prefix,
 // Emits the entries selected by (prefix, plen) to the row's output, in entry
 // order, reserving the slots with one atomic on the row's out_count -- or,
 // when the team is the row's only writer (sole), from slot 0 without it: the
-// atomic's round trip sits on the finish's critical path.
+// atomic's round trip sits on the finish's critical path.  Warp w owns a
+// contiguous run of entries and walks it 32 at a time (conflict-free smem
+// reads; a ballot ranks the selected lanes, so the writes coalesce).
 template <class Tm, int VT, bool SCALE, typename G>
 __device__ void smem_emit(const EngineParams& p, G get, int cnt, const RowCtx& rc, uint64_t prefix, int plen,
                           RowState* rs, Misc* m, bool sole = false) {
   using K = KT<VT, SCALE>;
   const int W = K::KB + rc.IB;
   const int sh = W - plen;
-  const int per = (cnt + Tm::kSize - 1) / Tm::kSize;
-  const int lo = min(cnt, Tm::tid() * per);
-  const int hi = min(cnt, lo + per);
-  uint32_t mine = 0;
-  for (int i = lo; i < hi; ++i) {
-    uint32_t bits;
-    int64_t pos;
+  const int lane = threadIdx.x & 31;
+  const int span = (cnt + Tm::kWarps * 32 - 1) / (Tm::kWarps * 32) * 32;
+  const int lo = min(cnt, Tm::wid() * span);
+  const int hi = min(cnt, lo + span);
+  auto selected = [&](int i, uint32_t& bits, int64_t& pos) -> bool {
+    if (i >= hi) return false;
     get(i, bits, pos);
     const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
-    mine += shr64(c, sh) <= prefix;
+    return shr64(c, sh) <= prefix;
+  };
+  uint32_t mine = 0;
+  for (int b = lo; b < hi; b += 32) {
+    uint32_t bits;
+    int64_t pos;
+    mine += (uint32_t)__popc(__ballot_sync(kFull, selected(b + lane, bits, pos)));
   }
   uint32_t total;
-  const uint32_t ex = block_excl_scan<Tm>(mine, m->scan, &total);
-  uint32_t base = 0;
+  const uint32_t ex = block_excl_scan<Tm>(lane == 0 ? mine : 0u, m->scan, &total);
+  uint32_t base = __shfl_sync(kFull, ex, 0);
   if (!sole) {
     if (Tm::tid() == 0) m->counter = total ? atomicAdd(reinterpret_cast<uint32_t*>(&rs->out_count), total) : 0u;
     Tm::sync();
-    base = m->counter;
+    base += m->counter;
   }
-  int64_t slot = (int64_t)base + ex;
-  for (int i = lo; i < hi; ++i) {
-    uint32_t bits;
-    int64_t pos;
-    get(i, bits, pos);
-    const uint64_t c = ((uint64_t)sel_key<VT, SCALE>(bits, rc.flip, rc.scaler) << rc.IB) | (uint64_t)pos;
-    if (shr64(c, sh) <= prefix) {
-      if (slot < rc.k) write_out<VT>(p, rc.out_off + slot, bits, pos);
-      ++slot;
-    }
+  for (int b = lo; b < hi; b += 32) {
+    uint32_t bits = 0;
+    int64_t pos = 0;
+    const bool s = selected(b + lane, bits, pos);
+    const unsigned bal = __ballot_sync(kFull, s);
+    const int64_t slot = (int64_t)base + __popc(bal & ((1u << lane) - 1u));
+    if (s && slot < rc.k) write_out<VT>(p, rc.out_off + slot, bits, pos);
+    base += (uint32_t)__popc(bal);
   }
   Tm::sync();
 }
@@ -1068,7 +1079,8 @@ __device__ inline void grid_barrier(Header* h, uint32_t spin_limit) {
     asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&h->bar_count) : "memory");
     const uint32_t target = (old / gridDim.x + 1u) * gridDim.x;
     uint32_t it = 0;
-    while (ld_acquire(&h->bar_count) < target) {
+    // the last arrival has seen every other one through its own atomic
+    while (old + 1u != target && ld_acquire(&h->bar_count) < target) {
       if (++it > spin_limit) {
         atomicOr(&h->status, kStatusTimeout);
         break;
@@ -1274,9 +1286,10 @@ struct Engine {
   }
 
   // ---- whole row in shared memory (n <= kSmemRowCap)
+  template <class Tm = SideTeam>
   __device__ void smem_row(int r, const RowCtx& rc) {
     uint32_t* vals = reinterpret_cast<uint32_t*>(smem);
-    for_range_v<SideTeam, ES, U>(
+    for_range_v<Tm, ES, U>(
         p.val_in, rc.in_off, 0, rc.n, [&](uint32_t bits, int64_t pos, bool ok) { if (ok) vals[pos] = bits; },
         [&](const uint4& x, int64_t pos0, bool ok) {
           if (ok) {
@@ -1284,7 +1297,7 @@ struct Engine {
             for (int e = 0; e < VEC; ++e) vals[pos0 + e] = vec_elem<ES>(x, e);
           }
         });
-    SideTeam::sync();
+    Tm::sync();
     const int kk = min(rc.n, rc.k);
     uint64_t prefix = 0;
     int plen = 0, krem = kk;
@@ -1292,10 +1305,10 @@ struct Engine {
       bits = vals[i];
       pos = i;
     };
-    smem_resolve<SideTeam, VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
+    smem_resolve<Tm, VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
                             &p.hdr->status);
-    smem_emit<SideTeam, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m, true);
-    post_process<SideTeam, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
+    smem_emit<Tm, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m, true);
+    post_process<Tm, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
   }
 
   // ---- one CTA, the whole row from global memory (n <= p.cta_cap)
@@ -1327,6 +1340,7 @@ struct Engine {
     });
   }
 
+  template <class Tm = SideTeam>
   __device__ void cta_row(int r, const RowCtx& rc) {
     RowState* rs = p.rs + r;
     uint64_t* ent = reinterpret_cast<uint64_t*>(smem);
@@ -1337,29 +1351,29 @@ struct Engine {
     };
     if ((int64_t)rc.k * kPrefRatio <= rc.n) {
       // pre-filter inside the CTA
-      const uint32_t T = sample_threshold<SideTeam>(rc);
-      if (SideTeam::tid() == 0) m->counter = 0;
-      SideTeam::sync();
+      const uint32_t T = sample_threshold<Tm>(rc);
+      if (Tm::tid() == 0) m->counter = 0;
+      Tm::sync();
       auto one = [&](uint32_t bits, int64_t pos, bool ok) {
         const bool hit = ok && key_of(bits, rc) <= T;
         if (!__any_sync(kFull, hit)) return;
         const uint32_t se = warp_reserve(hit ? 1u : 0u, &m->counter);
         if (hit && se < (uint32_t)kCapSB) ent[se] = make_entry(bits, pos);
       };
-      for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      for_range_v<Tm, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
       });
-      SideTeam::sync();
+      Tm::sync();
       const int c = (int)m->counter;
-      SideTeam::sync();
+      Tm::sync();
       if (c >= rc.k && c <= kCapSB) {
         uint64_t prefix = 0;
         int plen = 0, krem = rc.k;
-        smem_resolve<SideTeam, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+        smem_resolve<Tm, VT, SCALE>(get, c, rc, prefix, plen, krem, c, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                                 &p.hdr->status);
-        smem_emit<SideTeam, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m, true);
-        post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+        smem_emit<Tm, VT, SCALE>(p, get, c, rc, prefix, plen, rs, m, true);
+        post_process<Tm, VT, SCALE>(p, rc, smem, m);
         return;
       }
       // threshold missed: radix levels below
@@ -1371,43 +1385,43 @@ struct Engine {
     for (int guard = 0; guard < 16 && count != krem && count > kCapSB; ++guard) {
       const int D = min(12, W - plen);
       const int NB = 1 << D;
-      for (int i = SideTeam::tid(); i < NB; i += SideTeam::kSize) hist[i] = 0;
-      SideTeam::sync();
+      for (int i = Tm::tid(); i < NB; i += Tm::kSize) hist[i] = 0;
+      Tm::sync();
       const int sh = W - plen, sd = W - plen - D;
       const uint32_t dm = (uint32_t)NB - 1u;
       auto one = [&](uint32_t bits, int64_t pos, bool ok) {
         const uint64_t c = ((uint64_t)key_of(bits, rc) << rc.IB) | (uint64_t)pos;
         hist_add_agg(hist, (uint32_t)shr64(c, sd) & dm, ok && shr64(c, sh) == prefix);
       };
-      for_range_v<SideTeam, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
+      for_range_v<Tm, ES, U>(p.val_in, rc.in_off, 0, rc.n, one, [&](const uint4& x, int64_t pos0, bool ok) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) one(vec_elem<ES>(x, e), pos0 + e, ok);
       });
-      SideTeam::sync();
-      block_select<SideTeam, false>(hist, NB, (uint32_t)krem, m);
+      Tm::sync();
+      block_select<Tm, false>(hist, NB, (uint32_t)krem, m);
       if (!m->sel_found) {
-        if (SideTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
+        if (Tm::tid() == 0) atomicOr(&p.hdr->status, kStatusSelect);
         return;
       }
       prefix = (prefix << D) | m->sel_bin;
       plen += D;
       krem -= (int)m->sel_cum;
       count = (int)m->sel_cnt;
-      SideTeam::sync();
+      Tm::sync();
     }
     const bool final_mode = count == krem;
-    if (SideTeam::tid() == 0) m->counter = 0;
-    SideTeam::sync();
-    cta_filter(rc, rs, prefix, plen, final_mode, ent);
-    SideTeam::sync();
+    if (Tm::tid() == 0) m->counter = 0;
+    Tm::sync();
+    cta_filter<Tm>(rc, rs, prefix, plen, final_mode, ent);
+    Tm::sync();
     if (!final_mode) {
       const int ne = min((int)m->counter, kCapSB);
-      SideTeam::sync();
-      smem_resolve<SideTeam, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
+      Tm::sync();
+      smem_resolve<Tm, VT, SCALE>(get, ne, rc, prefix, plen, krem, ne, reinterpret_cast<uint32_t*>(smem + kResolveHistOff), m,
                               &p.hdr->status);
-      smem_emit<SideTeam, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
+      smem_emit<Tm, VT, SCALE>(p, get, ne, rc, prefix, plen, rs, m);
     }
-    post_process<SideTeam, VT, SCALE>(p, rc, smem, m);
+    post_process<Tm, VT, SCALE>(p, rc, smem, m);
   }
 
   // ---- copy chunk ia of a k >= n row (every element is selected)
@@ -2237,6 +2251,12 @@ __device__ __forceinline__ bool is_streaming(int kind, int isA, int fin) {
              : (!fin && (kind == kKindGridPref || kind == kKindGridRadix));
 }
 
+// Claims the next work item.  Items 0 .. gridDim.x - 1 are the CTAs' first
+// items, taken by block index without a claim; the counter hands out the rest.
+__device__ __forceinline__ int claim_item(const EngineParams& p) {
+  return (int)(gridDim.x + atomicAdd(&p.hdr->qhead, 1u));
+}
+
 // Producer (one thread): claims items in order, routes streaming items to
 // the consumer queue and the rest to the side queue, and issues the bulk
 // copies of each streaming chunk into the ring as slots drain.
@@ -2277,7 +2297,13 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       }
     }
   };
-  int q = first_q >= 0 ? first_q : (int)atomicAdd(&p.hdr->qhead, 1u);
+  int q = first_q >= 0 ? first_q : claim_item(p);
+  // Threshold word of the next chunk item's row, loaded while the current
+  // item's copies are issued (pf_row: its row, -1 = none).  The word holds
+  // the threshold itself, so a relaxed load suffices; a word read before the
+  // threshold existed is read again below.
+  int pf_row = -1;
+  uint64_t pf_tr = 0;
   while (true) {
     ItemDesc d{};
     if (q >= NQ) {
@@ -2298,17 +2324,24 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       // times the side team's threads): nothing streams after them.
       if (ir.fin && fin_tail > 0 && q >= NQ - fin_tail) push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
       else push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
+      if (q + 1 >= NQ) {  // the last item: every later claim falls past the end
+        q = NQ;
+        continue;
+      }
       throttle(q);
-      q = (int)atomicAdd(&p.hdr->qhead, 1u);
+      q = claim_item(p);
       continue;
     }
     if (!ir.isA && rc.kind == kKindGridPref) {
-      // The chunk is useless before its row's threshold exists, so its copies
-      // wait for it: at the start this keeps the ring fills of all CTAs from
-      // queueing ahead of the sample reads that produce the thresholds.  The
-      // sample item precedes the chunk in the claim order, so the wait ends.
-      uint64_t v = ld_acquire_u64(&p.rs[ir.row].tready);
-      for (uint32_t it = 0; !(v >> 32) && it < p.spin_limit; ++it) {
+      // The chunk is useless before its row's threshold exists, so in a large
+      // call its copies wait for it: at the start this keeps the ring fills of
+      // all CTAs from queueing ahead of the sample reads that produce the
+      // thresholds.  The sample item precedes the chunk in the claim order, so
+      // the wait ends.  A small call (early_copy) streams its few megabytes
+      // while the thresholds are computed; its consumers wait for them.
+      uint64_t v = ir.row == pf_row ? pf_tr : 0ull;
+      if (!(v >> 32)) v = ld_acquire_u64(&p.rs[ir.row].tready);
+      for (uint32_t it = 0; !(v >> 32) && !p.early_copy && it < p.spin_limit; ++it) {
         __nanosleep(128);
         v = ld_acquire_u64(&p.rs[ir.row].tready);
       }
@@ -2339,7 +2372,8 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     // issued: a claim made early holds an item that an idle CTA could start.
     const bool near_tail = fin_tail > 0 && q + 1 >= NQ - fin_tail;
     const bool late_claim = near_tail || q + 1 >= NQ - fin_tail - (int)gridDim.x;
-    int nq = late_claim ? -1 : (int)atomicAdd(&p.hdr->qhead, 1u);
+    const bool last = q + 1 >= NQ;
+    int nq = last ? NQ : late_claim ? -1 : claim_item(p);
     const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
     uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
     for (int i = 0; i < d.nst; ++i, ++g) {
@@ -2359,10 +2393,20 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       const uint32_t bytes = (uint32_t)min((int64_t)kStageVecs, nvec - v0) * 16u;
       mbar_expect_tx(&ctl->full[slot], bytes);
       bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &ctl->full[slot]);
+      if (i == d.nst / 2) {  // the claim has long returned: reading it does not stall the copies
+        pf_row = -1;
+        if (nq >= 0 && nq < NQ) {
+          const ItemRef nir = resolve_item(p, nq, NA, NB, lag, una, unc, ufin);
+          if (!nir.isA && !nir.fin) {
+            pf_row = nir.row;
+            pf_tr = ld_relaxed_u64(&p.rs[nir.row].tready);
+          }
+        }
+      }
     }
-    if (late_claim) {
+    if (late_claim && !last) {
       throttle(q);
-      nq = (int)atomicAdd(&p.hdr->qhead, 1u);
+      nq = claim_item(p);
     }
     q = nq;
   }
@@ -2429,12 +2473,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     lag = __ldcg(&p.hdr->lag);
     fin_tail = __ldcg(&p.hdr->fin_tail);
   }
-  // The CTA's first claim.  A pre-filter sample claimed here is computed by
-  // the whole CTA before the teams start: nothing streams until the first
-  // thresholds exist, so these samples are on every CTA's critical path.
-  if (threadIdx.x == 0) ctl->first_q = (int)atomicAdd(&p.hdr->qhead, 1u);
-  __syncthreads();
-  int first_q = ctl->first_q;
+  // The CTA's first item is its block index.  A pre-filter sample taken here
+  // is computed by the whole CTA before the teams start: nothing streams
+  // until the first thresholds exist, so these samples are on every CTA's
+  // critical path.
+  int first_q = (int)blockIdx.x;
   if (first_q < NA + NB) {
     const ItemRef ir = resolve_item(p, first_q, NA, NB, lag, una, unc, ufin);
     const RowCtx rc = load_row<VT, SCALE>(p, ir.row);

@@ -260,6 +260,16 @@ const char* radik_last_error(void);
 /* Library version as 10000 * major + 100 * minor + patch. */
 int radik_version(void);
 
+/* ---- Timeline build (libradik_b200_timeline.so, compiled with RADIK_TIMELINE)
+ * Engine launches made after this call write, per CTA, 32 slots of 64 bits
+ * into `stamps` (a device buffer of at least grid x 32 x 8 bytes, cleared by
+ * the caller): %globaltimer nanoseconds at the engine's phase boundaries
+ * (kernel start, first sample, consumer / side teams done, finish start and
+ * its steps, phase B, end) and, in slot 31, a finishing row's candidate count.
+ * radik_b200/timeline.py reads and summarises them.  Pass NULL to detach.
+ * The normal library returns RADIK_ENOTSUP. */
+int radik_timeline_attach(void* stamps);
+
 #ifdef __cplusplus
 }
 #endif

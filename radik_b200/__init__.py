@@ -89,6 +89,8 @@ def lib() -> ctypes.CDLL:
     L.radik_strerror.restype = ctypes.c_char_p
     L.radik_last_error.argtypes = []
     L.radik_last_error.restype = ctypes.c_char_p
+    L.radik_timeline_attach.argtypes = [vp]
+    L.radik_timeline_attach.restype = ctypes.c_int
     L.radik_version.argtypes = []
     for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
                  "radik_get_status", "radik_version", "radik_topk_static", "radik_autotune_ex", "radik_autotune_rows",

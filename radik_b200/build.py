@@ -15,6 +15,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libradik_b200.so")
+# The timeline build: the same sources with RADIK_TIMELINE, whose engine
+# writes per-CTA phase stamps (radik_timeline_attach, radik_b200/timeline.py).
+LIB_TIMELINE = os.path.join(HERE, "libradik_b200_timeline.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in (
     "radik_engine_f32.cu", "radik_engine_f16.cu", "radik_engine_bf16.cu", "radik_plan.cu", "radik_api.cu",
     "radik_server.cu", "radik_split.cu")]
@@ -47,21 +50,25 @@ def _stale(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_library(force: bool = False, verbose: bool = False) -> str:
-    """Compiles each translation unit in parallel, then links the .so."""
-    if not (force or _stale(LIB, SOURCES + HEADERS)):
-        return LIB
+def build_library(force: bool = False, verbose: bool = False, timeline: bool = False) -> str:
+    """Compiles each translation unit in parallel, then links the .so
+    (timeline=True: the timeline build, libradik_b200_timeline.so)."""
+    lib = LIB_TIMELINE if timeline else LIB
+    obj_dir = os.path.join(OBJ_DIR, "timeline") if timeline else OBJ_DIR
+    if not (force or _stale(lib, SOURCES + HEADERS)):
+        return lib
     from concurrent.futures import ThreadPoolExecutor
 
-    os.makedirs(OBJ_DIR, exist_ok=True)
+    os.makedirs(obj_dir, exist_ok=True)
     nvcc = _nvcc()
     inc = "-I" + os.path.join(ROOT, "include")
+    extra = ["-DRADIK_TIMELINE"] if timeline else []
 
     def compile_one(src: str) -> str:
-        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         if not force and not _stale(obj, [src] + HEADERS + [__file__]):
             return obj  # up to date: the engine units take minutes each
-        cmd = [nvcc, *NVCC_FLAGS, inc, "-c", "-o", obj, src]
+        cmd = [nvcc, *NVCC_FLAGS, *extra, inc, "-c", "-o", obj, src]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
@@ -70,10 +77,10 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(compile_one, SOURCES))
-    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs],
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib + ".tmp", *objs],
                    check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 CLI_SRC = os.path.join(HERE, "csrc", "radik_cli.cu")
@@ -116,9 +123,13 @@ def build_oracle(verbose: bool = False) -> None:
 
 def build(force: bool = False, verbose: bool = False) -> None:
     build_library(force=force, verbose=verbose)
+    build_library(force=force, verbose=verbose, timeline=True)
     build_cli(force=force, verbose=verbose)
     build_oracle(verbose=verbose)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    if "--timeline" in sys.argv:
+        build_library(force="--force" in sys.argv, verbose=True, timeline=True)
+    else:
+        build(force="--force" in sys.argv, verbose=True)

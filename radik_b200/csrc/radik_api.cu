@@ -10,6 +10,7 @@
 #include "radik_b200.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -255,6 +256,9 @@ int check_common(int dtype, uint32_t flags, const void* val_in, const void* idx_
   return RADIK_OK;
 }
 
+// Device buffer of the timeline build's per-CTA phase stamps (null: none).
+std::atomic<unsigned long long*> g_timeline{nullptr};
+
 EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, void* idx_out, uint8_t* ws,
                          const Layout& L, int B, const Config& c, uint32_t flags) {
   EngineParams p{};
@@ -279,6 +283,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.S = kSlots;
   p.flags = flags;
   p.spin_limit = kSpinLimit;
+  p.timeline = g_timeline.load();
   return p;
 }
 
@@ -582,6 +587,16 @@ using namespace radik;
 extern "C" {
 
 int radik_version(void) { return 100; }
+
+int radik_timeline_attach(void* stamps) {
+#ifdef RADIK_TIMELINE
+  g_timeline.store(static_cast<unsigned long long*>(stamps));
+  return RADIK_OK;
+#else
+  (void)stamps;
+  return fail(RADIK_ENOTSUP, "radik_timeline_attach: this library was built without RADIK_TIMELINE");
+#endif
+}
 
 const char* radik_last_error(void) { return g_last_error.c_str(); }
 

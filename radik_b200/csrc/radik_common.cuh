@@ -176,6 +176,7 @@ struct EngineParams {
   int32_t fin_delay;        // uniform mode: rows a FIN item trails its row
   uint32_t flags;
   uint32_t spin_limit;      // iterations of a bounded wait
+  unsigned long long* timeline;  // per-CTA phase stamps (timeline build only; else null)
   // uniform mode: every row has n = u_n, k = u_k, contiguous input,
   // output at r * u_k.
   int32_t uniform;

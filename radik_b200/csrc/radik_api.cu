@@ -148,6 +148,8 @@ int env_int(const char* name, int dflt) {
 struct Config {
   int CH, CHR, D1, cta_cap;
   int early_copy;  // chunk copies may start before their row's threshold exists
+  int l2_ahead;    // ring stages a chunk's L2 prefetch runs ahead of its copies
+  int tail_div;    // the last rows' pre-filter chunks are CH / tail_div long (1: no split)
 };
 
 // A tuned shape bucket: a field of 0 keeps the built-in choice.
@@ -239,6 +241,16 @@ Config choose_config(int64_t stream_elems, int grid, const Tuned& t, int es, int
   c.early_copy = stream_elems * es <= ((int64_t)64 << 20) ? 1 : 0;
   const int eec = env_int("RADIK_EARLY", -1);
   if (eec == 0 || eec == 1) c.early_copy = eec;
+  // An L2 prefetch two stages ahead of the ring's copies: 256 x 2^20 fp32
+  // k = 256 / 1024 / 32: 202 / 230 / 196 us without, 196 / 226 / 191 us with
+  // it; farther ahead is slower (16 stages: 212 us), and 16-bit rows gain
+  // nothing (156 us at 0, 1 or 2 stages).
+  c.l2_ahead = es == 4 ? 2 : 0;
+  c.tail_div = 1;
+  const int etd = env_int("RADIK_TAIL_DIV", 0);
+  if (etd >= 1 && etd <= 8) c.tail_div = etd;
+  const int ela = env_int("RADIK_L2_AHEAD", -1);
+  if (ela >= 0 && ela <= 64) c.l2_ahead = ela;
   return c;
 }
 
@@ -280,6 +292,7 @@ EngineParams base_params(const void* val_in, const void* idx_in, void* val_out, 
   p.D1 = c.D1;
   p.cta_cap = c.cta_cap;
   p.early_copy = c.early_copy;
+  p.l2_ahead = c.l2_ahead;
   p.S = kSlots;
   p.flags = flags;
   p.spin_limit = kSpinLimit;
@@ -400,17 +413,29 @@ int launch_call(int dtype, uint32_t flags, const void* val_in, const void* idx_i
     p.u_cand_cap = row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
-    // B sequence layout (see uniform_b_item) and the lag it needs
+    // B sequence layout (see UniformB) and the lag it needs
     const int64_t una = row_na(kind, n, cfg.CH, cfg.CHR), nc = row_nbc(kind, n, cfg.CH, cfg.CHR);
     const int64_t f = row_fin(kind);
     const int D = fin_delay_uniform((int)nc, grid);
     const int64_t Dd = std::min<int64_t>(D, B);
-    auto b0 = [&](int64_t q) { return q < Dd ? q * nc : Dd * nc + (q - Dd) * (nc + f); };
+    // Pre-filter rows in a call of several chunk waves: the last rows take
+    // chunks of half the length, so the last items of the claim order are
+    // short and the CTAs run out of work together.
+    int tail_rows = 0, ch_tail = cfg.CH;
+    if (kind == kKindGridPref && cfg.tail_div > 1 && (int64_t)B * nc >= 4LL * grid) {
+      ch_tail = std::max(kMinCH, (cfg.CH / cfg.tail_div + 31) / 32 * 32);
+      const int nct = ceil_div32(n, ch_tail);
+      tail_rows = (int)std::min<int64_t>(B - Dd, (3LL * grid + 2LL * nct - 1) / (2LL * nct));
+      if (tail_rows < 1 || nct <= nc) tail_rows = 0;
+    }
+    p.u_tail_rows = tail_rows;
+    p.u_ch_tail = ch_tail;
+    const UniformB ub{B, (int32_t)nc, tail_rows ? ceil_div32(n, ch_tail) : (int32_t)nc, tail_rows, (int32_t)f, D};
     int64_t maxlag = 0;
     for (int64_t r = 0; r < B && (nc > 0 || f); ++r) {
       int64_t first_b;
-      if (nc > 0) first_b = b0(r);
-      else first_b = (r + Dd < B) ? b0(r + Dd) + nc : (int64_t)B * nc + f * (B - Dd) + (r - (B - Dd));
+      if (nc > 0) first_b = ub.first(r);
+      else first_b = (r + Dd < B) ? ub.first(r + Dd) + nc : ub.first(B) + (r - (B - Dd));
       maxlag = std::max(maxlag, (r + 1) * una - first_b);
     }
     p.fin_delay = D;

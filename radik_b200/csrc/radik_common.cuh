@@ -171,6 +171,7 @@ struct EngineParams {
   int32_t D1;               // first digit width of histogram rows
   int32_t cta_cap;          // rows of up to this many keys are selected by one CTA
   int32_t early_copy;       // chunk copies may start before their row's threshold exists
+  int32_t l2_ahead;         // ring stages a chunk's L2 prefetch runs ahead of its copies (0: none)
   int32_t S;                // hist ring slots
   int32_t lag;              // uniform mode: A-ahead-of-B distance
   int32_t fin_delay;        // uniform mode: rows a FIN item trails its row
@@ -184,6 +185,8 @@ struct EngineParams {
   int32_t u_k;
   int32_t u_cand_cap;
   int64_t u_sort_cap;       // sort-scratch entries per row (0 if none)
+  int32_t u_tail_rows;      // the last rows, whose pre-filter chunks are u_ch_tail long (0: none)
+  int32_t u_ch_tail;
 };
 
 // ----------------------------------------------------------------------------
@@ -238,37 +241,56 @@ __host__ __device__ inline int32_t row_fin_wait(int kind, int32_t n, int32_t CH,
   return kind == kKindAll ? row_na(kind, n, CH, CHR) : row_nbc(kind, n, CH, CHR);
 }
 
-// B item decode for uniform batches (B rows, nc chunk items each, f = has
-// FIN, FINs delayed by D rows).  Sets row, sub (chunk index) and fin.
-__host__ __device__ inline void uniform_b_item(int64_t j, int32_t B, int32_t nc, int32_t f, int32_t D, int32_t* row,
-                                               int32_t* sub, int32_t* fin) {
-  const int64_t Dd = D < B ? D : B;
-  const int64_t head = Dd * nc;
-  const int64_t body = (int64_t)B * nc + (int64_t)f * (B - Dd);
-  if (j < head) {
-    *row = (int32_t)(j / nc);
-    *sub = (int32_t)(j % nc);
-    *fin = 0;
-  } else if (j < body) {
-    const int64_t jj = j - head;
-    const int64_t blk = nc + f;
-    const int64_t r = Dd + jj / blk;
-    const int64_t sb = jj % blk;
-    if (sb < nc) {
+// B items of an equal-length call.  Rows [0, B - R) have nc chunk items,
+// the last R rows nct (shorter chunks: the last items of the claim order are
+// short, so the CTAs run out of work together), and a row's FIN item (f = 1)
+// trails it by D rows.  Order: the chunks of rows [0, D); then, for each row
+// r in [D, B), its chunks followed by row r - D's FIN; then the FINs of rows
+// [B - D, B).
+struct UniformB {
+  int32_t B, nc, nct, R, f, D;
+  __host__ __device__ int32_t chunks(int64_t r) const { return r >= (int64_t)B - R ? nct : nc; }
+  __host__ __device__ int64_t dd() const { return D < B ? D : B; }
+  // B index of row r's first chunk (r = B: the first tail FIN)
+  __host__ __device__ int64_t first(int64_t r) const {
+    const int64_t s = (int64_t)B - R;
+    const int64_t head = r < s ? r : s;
+    int64_t idx = head * nc + (r - head) * nct;
+    if (r > dd()) idx += (int64_t)f * (r - dd());
+    return idx;
+  }
+  __host__ __device__ int64_t count() const { return first(B) + (int64_t)f * dd(); }
+  // item j -> row, chunk index (sub) and whether it is a FIN
+  __host__ __device__ void decode(int64_t j, int32_t* row, int32_t* sub, int32_t* fin) const {
+    const int64_t Dd = dd(), s = (int64_t)B - R;
+    const int64_t end = first(B);
+    if (j >= end) {
+      *row = (int32_t)((int64_t)B - Dd + (j - end));
+      *sub = 0;
+      *fin = 1;
+      return;
+    }
+    // rows fall in three runs of equal block size: [0, lo), [lo, hi), [hi, B)
+    const int64_t lo = Dd < s ? Dd : s, hi = Dd < s ? s : Dd;
+    const int64_t starts[3] = {0, lo, hi};
+    int k = 2;
+    if (j < first(hi)) k = 1;
+    if (j < first(lo)) k = 0;
+    const int64_t r0 = starts[k];
+    const int64_t size = chunks(r0) + (r0 >= Dd ? f : 0);
+    const int64_t r = r0 + (j - first(r0)) / size;
+    const int64_t o = (j - first(r0)) % size;
+    if (o < chunks(r)) {
       *row = (int32_t)r;
-      *sub = (int32_t)sb;
+      *sub = (int32_t)o;
       *fin = 0;
     } else {
       *row = (int32_t)(r - Dd);
       *sub = 0;
       *fin = 1;
     }
-  } else {
-    *row = (int32_t)((int64_t)B - Dd + (j - body));
-    *sub = 0;
-    *fin = 1;
   }
-}
+};
 
 // Candidate region capacity of a row: enough for the smem finisher's set or
 // one eighth of the row, whichever is larger (never more than n).

@@ -63,7 +63,8 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kTlSlots = 32;
 enum TlSlot : int {
   kTlStart = 0, kTlFirstSample = 1, kTlConsDone = 2, kTlSideDone = 3, kTlFinEnd = 4, kTlPhaseB = 5, kTlEnd = 6,
-  kTlFinStart = 7, kTlSampleIn = 8, kTlItemStart = 14, kTlChunkEnd = 15, kTlFinBegin = 16, kTlFinLoaded = 17,
+  kTlFinStart = 7, kTlSampleIn = 8, kTlSampleIssue = 9, kTlSampleKeys = 10, kTlItemStart = 14, kTlChunkEnd = 15,
+  kTlFinBegin = 16, kTlFinLoaded = 17,
   kTlFinResolved = 18, kTlFinEmitted = 19, kTlFinPost = 20, kTlFinCands = 31
 };
 #ifdef RADIK_TIMELINE
@@ -170,6 +171,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+}
+
+// Prefetch of [src, src + bytes) into L2 (both 16-byte multiples; this GPU's
+// memory only).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
 // ----------------------------------------------------------------------------
@@ -520,7 +527,11 @@ __device__ __forceinline__ RowCtx load_row(const EngineParams& p, int r) {
   }
   c.IB = index_bits(c.n);
   c.ch = row_chunk(c.kind, p.CH, p.CHR);
-  c.fin_wait = row_fin_wait(c.kind, c.n, p.CH, p.CHR);
+  if (p.uniform && p.u_tail_rows > 0 && c.kind == kKindGridPref && r >= p.B - p.u_tail_rows) {
+    c.ch = p.u_ch_tail;  // the short chunks at the end of the claim order
+    c.nbc = row_nbc(c.kind, c.n, c.ch, p.CHR);
+  }
+  c.fin_wait = c.kind == kKindAll ? c.na : c.nbc;
   c.flip = (p.flags & kFlagLargest) ? KT<VT, SCALE>::KMASK : 0u;
   c.scaler = 0.f;
   if constexpr (SCALE) {
@@ -1277,6 +1288,7 @@ struct Engine {
     // line i sits at first + floor(i * (nfull - 1) / (nlines - 1)), stepped in
     // 32.32 fixed point (one division per thread instead of one per line)
     const uint64_t step = nlines > 1 ? ((uint64_t)(nfull - 1) << 32) / (uint64_t)(nlines - 1) : 0;
+    if (Tm::kSize == FullTeam::kSize && Tm::tid() == 0) RADIK_TL(p, kTlSampleIssue);
     for (int j = Tm::tid(); j < 8 * nlines; j += Tm::kSize) {
       const int i = j >> 3;
       const int64_t line = first + (int64_t)(((uint64_t)i * step) >> 32);
@@ -1308,6 +1320,7 @@ struct Engine {
     }
     const uint64_t lo = lo32 == 0xFFFFFFFFu && hi32 == 0 ? ~0ull : (uint64_t)lo32, hi = hi32;
     Tm::sync();
+    if (Tm::kSize == FullTeam::kSize && Tm::tid() == 0) RADIK_TL(p, kTlSampleKeys);
     uint32_t* hist = reinterpret_cast<uint32_t*>(big ? scratch + S * 4 : smem + kSampleHistOff);  // behind the keys
     const uint32_t t = block_sample_threshold<Tm, K::KB>(keys, S, sample_rank(rc.n, rc.k, S), lo, hi, hist, m,
                                                          &p.hdr->status);
@@ -2268,6 +2281,13 @@ __device__ __forceinline__ bool decode_item(int q, int NA, int NB, int L, int& i
 }
 
 // Item geometry of a claim: which row, A or B item, chunk, FIN.
+// The B-item layout of an equal-length call (see UniformB).
+__device__ __forceinline__ UniformB uniform_b(const EngineParams& p, int unc, int ufin) {
+  const int R = p.u_tail_rows;
+  const int nct = R > 0 ? (int)ceil_div32(p.u_n, p.u_ch_tail) : unc;
+  return UniformB{p.B, unc, nct, R, ufin, p.fin_delay};
+}
+
 struct ItemRef {
   int32_t row, sub, isA, fin;
 };
@@ -2281,7 +2301,7 @@ __device__ __forceinline__ ItemRef resolve_item(const EngineParams& p, int q, in
     it.row = p.uniform ? idx / una : p.a_row[idx];
     it.sub = idx;  // made row-relative once the row's a0 is known
   } else if (p.uniform) {
-    uniform_b_item(idx, p.B, unc, ufin, p.fin_delay, &it.row, &it.sub, &it.fin);
+    uniform_b(p, unc, ufin).decode(idx, &it.row, &it.sub, &it.fin);
   } else {
     const int32_t v = p.b_row[idx];
     it.row = v & 0x7FFFFFFF;
@@ -2421,6 +2441,12 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     int nq = last ? NQ : late_claim ? -1 : claim_item(p);
     const uint4* src = reinterpret_cast<const uint4*>(row + d.va * ES);
     uint4* ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ctl) - (kCtrlOff + 6144));
+    // L2 prefetch p.l2_ahead stages ahead of the copies: the ring's copies
+    // then wait for L2 rather than DRAM, and more of the row is in flight
+    // than the ring holds.
+    const int ahead = p.l2_ahead;
+    auto stage_bytes = [&](int i) { return (uint32_t)min((int64_t)kStageVecs, nvec - (int64_t)i * kStageVecs) * 16u; };
+    for (int i = 0; i < min(ahead, d.nst); ++i) bulk_prefetch_l2(src + (int64_t)i * kStageVecs, stage_bytes(i));
     for (int i = 0; i < d.nst; ++i, ++g) {
       constexpr uint32_t NS = ring_stages<VT>();
       const uint32_t slot = g % NS;
@@ -2435,9 +2461,10 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
         }
       }
       const int64_t v0 = (int64_t)i * kStageVecs;
-      const uint32_t bytes = (uint32_t)min((int64_t)kStageVecs, nvec - v0) * 16u;
+      const uint32_t bytes = stage_bytes(i);
       mbar_expect_tx(&ctl->full[slot], bytes);
       bulk_g2s(ring + (size_t)slot * kStageVecs, src + v0, bytes, &ctl->full[slot]);
+      if (ahead > 0 && i + ahead < d.nst) bulk_prefetch_l2(src + (int64_t)(i + ahead) * kStageVecs, stage_bytes(i + ahead));
       if (i == d.nst / 2) {  // the claim has long returned: reading it does not stall the copies
         pf_row = -1;
         if (nq >= 0 && nq < NQ) {
@@ -2510,7 +2537,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     unc = row_nbc(kind, p.u_n, p.CH, p.CHR);
     ufin = row_fin(kind);
     NA = p.B * una;
-    NB = p.B * (unc + ufin);
+    NB = (int)uniform_b(p, unc, ufin).count();
     lag = p.lag;
     fin_tail = ufin ? min(p.fin_delay, p.B) : 0;
   } else {

@@ -15,7 +15,9 @@ device buffer (radik_timeline_attach).  For each shape it
 A shape is dtype:rows:n:k (largest, unsorted, U(0,1) values).  The phases:
 
   start          kernel entry
+  sample_issue   a whole-CTA sample starts its copies
   sample_in      a whole-CTA sample's keys are in shared memory
+  sample_keys    ... and are converted to selection keys
   first_sample   that sample's threshold is published
   item_start     a consumer team starts its last item (its threshold seen)
   chunk_end      a consumer team ends its last pre-filter chunk
@@ -40,7 +42,8 @@ import os
 import sys
 
 SLOTS = 32
-PHASES = {0: "start", 8: "sample_in", 1: "first_sample", 14: "item_start", 15: "chunk_end", 2: "cons_done",
+PHASES = {0: "start", 9: "sample_issue", 8: "sample_in", 10: "sample_keys", 1: "first_sample", 14: "item_start",
+          15: "chunk_end", 2: "cons_done",
           3: "side_done", 7: "fin_start", 16: "fin_begin", 17: "fin_loaded", 18: "fin_resolved",
           19: "fin_emitted", 20: "fin_post", 4: "fin_end", 5: "phase_b", 6: "end"}
 CANDS_SLOT = 31

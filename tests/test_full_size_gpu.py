@@ -178,6 +178,8 @@ F32_SPECIAL = np.array([0x7FC00000, 0x7F800001, 0x7FFFFFFF, 0xFFC00000, 0xFF8000
                         0x00000000, 0x80000000, 0x00000001, 0x80000001], dtype=np.uint32)
 F16_SPECIAL = np.array([0x7E00, 0x7C01, 0x7FFF, 0xFE00, 0x7C00, 0xFC00, 0x0000, 0x8000, 0x0001, 0x8001],
                        dtype=np.uint16)
+BF16_SPECIAL = np.array([0x7FC0, 0x7F81, 0x7FFF, 0xFFC0, 0x7F80, 0xFF80, 0x0000, 0x8000, 0x0001, 0x8001],
+                        dtype=np.uint16)
 
 
 def edge_row(n, seed, dtype, frac):
@@ -188,15 +190,29 @@ def edge_row(n, seed, dtype, frac):
     if dtype == rk.F16:
         b = x.astype(np.float16).view(np.uint16).copy()
         sp = F16_SPECIAL
+    elif dtype == rk.BF16:
+        b = workloads.to_bf16_bits(x).copy()
+        sp = BF16_SPECIAL
     else:
         b = x.view(np.uint32).copy()
         sp = F32_SPECIAL
     pos = g.random(n) < frac
     b[pos] = sp[g.integers(0, len(sp), int(pos.sum()))]
-    return b.view(np.float16 if dtype == rk.F16 else np.float32)
+    return b.view(np.float16) if dtype == rk.F16 else b if dtype == rk.BF16 else b.view(np.float32)
 
 
-@pytest.mark.parametrize("dtype", [rk.F32, rk.F16], ids=["f32", "f16"])
+def _to_dev(flat, dtype):
+    t = torch.from_numpy(np.ascontiguousarray(flat))
+    return (t.view(torch.bfloat16) if dtype == rk.BF16 else t).to(DEV)
+
+
+def _host_values(gv, dtype):
+    gv = gv.view(torch.int16) if dtype == rk.BF16 else gv
+    v = gv.cpu().numpy().reshape(-1)
+    return v.view(np.uint16) if dtype == rk.BF16 else v
+
+
+@pytest.mark.parametrize("dtype", [rk.F32, rk.F16, rk.BF16], ids=["f32", "f16", "bf16"])
 @pytest.mark.parametrize("B,n,k", [(1, 100000, 300), (4, 1 << 20, 256), (1, 1 << 20, 20000), (1, 1 << 22, 4096),
                                    (3, 5000, 77)])
 @pytest.mark.parametrize("frac", [0.002, 0.3])
@@ -207,23 +223,30 @@ def test_nan_zero_inf_rows_match_oracle(dtype, B, n, k, frac):
     -inf.  (RadiK instead skips NaN in its first histogram and compares
     floats in its filter: radik/RadixSelect/radixselect_l.cuh:189-194.)"""
     flat = np.concatenate([edge_row(n, 300 + r, dtype, frac) for r in range(B)])
-    t = torch.from_numpy(flat).to(DEV)
+    t = _to_dev(flat, dtype)
     for largest, sorted_ in ((True, False), (False, True), (True, True)):
         gv, gi = rk.topk(t, k, [n] * B, largest=largest, sorted=sorted_)
-        want = oracle.topk(flat, [n] * B, k, flags=oracle.flags_of(largest, sorted_))
-        assert_same_selection((gv.cpu().numpy().reshape(-1), gi.cpu().numpy().reshape(-1)), want, [n] * B, [k] * B,
+        want = oracle.topk(flat, [n] * B, k, flags=oracle.flags_of(largest, sorted_), dtype=dtype)
+        assert_same_selection((_host_values(gv, dtype), gi.cpu().numpy().reshape(-1)), want, [n] * B, [k] * B,
                               [r * k for r in range(B)], sorted_, f"largest={largest} sorted={sorted_}")
 
 
+@pytest.mark.parametrize("dtype", [rk.F32, rk.F16, rk.BF16], ids=["f32", "f16", "bf16"])
 @pytest.mark.parametrize("largest", [True, False])
-def test_signed_zero_rows(largest):
+def test_signed_zero_rows(dtype, largest):
+    """Rows of +-0 (with a few +-1 for the 16-bit hit path): the threshold
+    lands on a zero, where float compares do not give the key order."""
     n = 300000
     g = workloads.rng(5)
     x = np.where(g.random(n) < 0.5, np.float32(0.0), np.float32(-0.0)).astype(np.float32)
-    t = torch.from_numpy(x).to(DEV)
+    u = g.random(n)
+    x[u < 0.0005] = 1.0
+    x[(u >= 0.0005) & (u < 0.001)] = -1.0
+    flat = x.astype(np.float16) if dtype == rk.F16 else workloads.to_bf16_bits(x) if dtype == rk.BF16 else x
+    t = _to_dev(flat, dtype)
     gv, gi = rk.topk(t, 1000, [n], largest=largest, sorted=True)
-    want = oracle.topk(x, [n], 1000, flags=oracle.flags_of(largest, True))
-    assert_same_selection((gv.cpu().numpy().reshape(-1), gi.cpu().numpy().reshape(-1)), want, [n], [1000], [0], True)
+    want = oracle.topk(flat, [n], 1000, flags=oracle.flags_of(largest, True), dtype=dtype)
+    assert_same_selection((_host_values(gv, dtype), gi.cpu().numpy().reshape(-1)), want, [n], [1000], [0], True)
 
 
 @pytest.mark.parametrize("B,n,k", [(4, 1 << 20, 256), (1, 1 << 22, 4096), (8, 200000, 1000)])

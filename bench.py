@@ -709,9 +709,11 @@ def run_serving(args, dev, stream, peak, peak_kind, requests=10000, rates=(1000,
             out_idx.fill_(-2)
             with rk.Server(dev.index, mode=mode, max_n=1 << 24, max_k=1024, budget_bytes=40 << 30) as srv:
                 srv.run_trace(items[:16])  # warm-up through the same server
+                st0 = srv.stats()
                 t0 = time.perf_counter()
                 lat = np.asarray(srv.run_trace(items), dtype=np.float64)
                 wall = time.perf_counter() - t0
+                st1 = srv.stats()
             torch.cuda.synchronize(dev)
             verify()
             span_s = max(float(np.max(arr + lat)) / 1e6, 1e-9)
@@ -719,9 +721,14 @@ def run_serving(args, dev, stream, peak, peak_kind, requests=10000, rates=(1000,
                          "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 4),
                          "throughput_rps": round(R / span_s, 1),
                          "gkeys_per_s": round(keys_total / span_s / 1e9, 3), "wall_s": round(wall, 3)}
+            if mode == 0:
+                row[name]["batches"] = st1["batches"] - st0["batches"]
+                row[name]["batches_beside_others"] = st1["batches_beside_others"] - st0["batches_beside_others"]
+                row[name]["max_batches_in_flight"] = st1["max_batches_in_flight"]
         row["p99_speedup_vs_per_request"] = round(row["per_request"]["p99_ms"] / max(row["batched"]["p99_ms"], 1e-9), 2)
         table.append(row)
     top = table[-1]["batched"]
+    sbs = side_by_side(dev)
     return {"workload": "serving: Poisson arrivals at 1k-50k req/s, n in {32000, 128256, 2^20, 2^24} w.p. "
                         "{.4,.3,.2,.1}, k in {1, 50, 1024}, 25% fp16, largest, unsorted, 40 GiB budget",
             "requests_per_rate": R, "latency": "submission to completion seen by the server's worker",
@@ -729,7 +736,85 @@ def run_serving(args, dev, stream, peak, peak_kind, requests=10000, rates=(1000,
             "gkeys_per_s_at_top_rate": top["gkeys_per_s"],
             "parity": {"requests": checked, "exact": bad == 0, "mismatched": bad,
                        "checked": "every request vs oracle on its own row (values bit-exact, index sets)"},
+            "side_by_side": sbs,
             "rates": table}
+
+
+def side_by_side(dev, reps=20):
+    """Two batches of the serving mix on two streams, as the server runs them:
+    A = one 2^24-key fp32 request (k = 1024) on three quarters of the SMs,
+    B = 16 requests of 32000 keys (k = 50) on the rest
+    (radik_topk_rows_ctas).  Times each alone and both launched together (CUDA
+    events from one origin event; medians of `reps`).  Together about equal
+    to the longer one alone means the two selections ran at the same time;
+    B's completion beside A shows a small batch not waiting for a large one.
+    Both outputs are checked against the oracle."""
+    import torch
+
+    import oracle
+    import radik_b200 as rk
+    from radik_b200 import workloads
+
+    total = rk.engine_ctas(dev.index)
+    a_ctas = total * 3 // 4
+    b_ctas = total - a_ctas
+    xa = workloads.normal(1 << 24, 61)
+    xb = workloads.normal(16 * 32000, 62)
+    ta, tb = torch.from_numpy(xa).to(dev), torch.from_numpy(xb).to(dev)
+    rows_a = [(0, 0, 1 << 24, 1024)]
+    rows_b = [(j * 32000, j * 50, 32000, 50) for j in range(16)]
+    sa, sb = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    res = {}
+
+    def run(which):
+        e0 = torch.cuda.Event(enable_timing=True)
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sa)
+        sb.wait_event(e0)
+        out = {}
+        if "a" in which:
+            out["a"] = rk.topk_rows(ta, rows_a, max_ctas=a_ctas, stream=sa, check=False)
+        if "b" in which:
+            out["b"] = rk.topk_rows(tb, rows_b, max_ctas=b_ctas, stream=sb, check=False)
+        ea.record(sa)
+        eb.record(sb)
+        return e0, ea, eb, out
+
+    for which in ("a", "b", "ab"):
+        for _ in range(3):
+            run(which)
+        torch.cuda.synchronize(dev)
+        marks = [run(which) for _ in range(reps)]
+        torch.cuda.synchronize(dev)
+        ta_us = [e0.elapsed_time(ea) * 1e3 for e0, ea, _, _ in marks]
+        tb_us = [e0.elapsed_time(eb) * 1e3 for e0, _, eb, _ in marks]
+        if which == "a":
+            res["a_alone_us"] = round(statistics.median(ta_us), 1)
+        elif which == "b":
+            res["b_alone_us"] = round(statistics.median(tb_us), 1)
+        else:
+            res["together_us"] = round(statistics.median([max(x, y) for x, y in zip(ta_us, tb_us)]), 1)
+            res["b_done_beside_a_us"] = round(statistics.median(tb_us), 1)
+            last = marks[-1][3]
+    res["serial_sum_us"] = round(res["a_alone_us"] + res["b_alone_us"], 1)
+    res["overlap_ratio"] = round(res["serial_sum_us"] / max(res["together_us"], 1e-9), 3)
+    res["ctas"] = {"a": a_ctas, "b": b_ctas, "device": total}
+    bad = 0
+    for x, rows, got in ((xa, rows_a, last["a"]), (xb, rows_b, last["b"])):
+        ns, ks, oo = [r[2] for r in rows], [r[3] for r in rows], [r[1] for r in rows]
+        ov, oi = oracle.topk(x, ns, ks, flags=oracle.flags_of(True, False), out_offsets=oo)
+        gv, gi = _bits(got[0].cpu().numpy()), got[1].cpu().numpy().astype(np.int64)
+        ov = _bits(ov)
+        for n, k, o in zip(ns, ks, oo):
+            a = np.argsort(gi[o:o + k], kind="stable")
+            b = np.argsort(oi[o:o + k], kind="stable")
+            if not (np.array_equal(gi[o:o + k][a], oi[o:o + k][b].astype(np.int64))
+                    and np.array_equal(gv[o:o + k][a], ov[o:o + k][b])):
+                bad += 1
+    res["parity"] = {"rows": len(rows_a) + len(rows_b), "exact": bad == 0, "mismatched_rows": bad}
+    res["note"] = ("A: one 2^24-key fp32 row, k=1024, on %d CTAs; B: 16 rows of 32000, k=50, on %d CTAs; "
+                   "overlap_ratio = (A alone + B alone) / together" % (a_ctas, b_ctas))
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -837,7 +922,7 @@ def main():
                             "d2h_bytes_per_step": 0, "note": "device-resident inputs"},
                     "roofline": r.get("roofline"), "clocks": clocks, "impl": impl.name,
                     "gpu_launches": None, wl: r})
-        ok = r.get("parity", {}).get("exact", True)
+        ok = r.get("parity", {}).get("exact", True) and r.get("side_by_side", {}).get("parity", {}).get("exact", True)
         emit(out)
         if world > 1:
             dist.barrier()
@@ -920,7 +1005,7 @@ def main():
         torch.cuda.empty_cache()
         if impl.name == "radik_b200":
             out["serving"] = run_serving(args, dev, stream, peak, peak_kind, args.serving_requests)
-            ok = ok and out["serving"]["parity"]["exact"]
+            ok = ok and out["serving"]["parity"]["exact"] and out["serving"]["side_by_side"]["parity"]["exact"]
         else:
             out["serving"] = {"unavailable": "the reference has no serving loop; its per-request form is the "
                                              "mode-1 baseline in the radik_b200 line"}

@@ -92,6 +92,19 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
                     void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
                     int task_num, int64_t total_n, int n_max, int k_max, void* stream);
 
+/* radik_topk_rows on at most max_ctas SMs (0: the whole device; the engine
+ * runs one CTA per SM).  Calls on different streams whose grids add up to at
+ * most the SM count run side by side on the device; the serving loop sizes
+ * its batches this way.  No RadiK counterpart: RadiK sizes its grid from the
+ * shape alone (topk_radixselect.h:117-130). */
+int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                         void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                         int task_num, int64_t total_n, int n_max, int k_max, int max_ctas, void* stream);
+
+/* Engine CTAs a call on the current device can use at most (one per SM):
+ * the limit that radik_topk_rows_ctas calls share. */
+int radik_engine_ctas(int* ctas);
+
 /* Synchronises the stream and returns the status of the last call made with
  * this workspace (RADIK_OK, RADIK_ETIMEOUT, RADIK_EINTERNAL, RADIK_EWORKSPACE).
  * device_bits (nullable) receives the raw device status word. */
@@ -200,8 +213,11 @@ int radik_shard_collect(int dtype, uint32_t flags, const void* val_in, int64_t n
  * staging, a stream each) and a device-memory budget.  Each request is one
  * row already on the device; its results land in the request's own device
  * buffers.  Requests that arrive while batches run are admitted into the next
- * batch as a slot and budget allow, so several batches are in flight at once
- * and their copies, planning and selection overlap on the device.  Each
+ * batch as a slot, the budget and free SMs allow: a batch asks for one engine
+ * CTA (one SM) per 2^16 keys, at most three quarters of the device when
+ * several slots exist, and starts when that many SMs are free of other
+ * batches.  So several batches are in flight at once and their selection
+ * kernels run side by side on disjoint SMs.  Each
  * batch is one radik_topk_rows launch over the requests of one (dtype, flags)
  * group; a request's result does not depend on the batch it joined (the
  * selection is exact, ties go to the lowest positions). */
@@ -235,6 +251,17 @@ typedef struct {
   void* idx_out;       /* device, k indices */
 } radik_trace_item;
 
+/* Counters of a server's batches since it was created. */
+typedef struct {
+  int64_t batches;                /* batches launched */
+  int64_t requests;               /* requests in them */
+  int64_t batches_beside_others;  /* batches launched while another batch was still in flight */
+  int32_t max_batches_in_flight;  /* most batches in flight at once */
+  int32_t max_ctas_in_flight;     /* most engine CTAs (SMs) held by batches at once */
+  int32_t ctas_total;             /* engine CTAs of the device (one per SM) */
+  int32_t ctas_cap;               /* most CTAs one batch may take */
+} radik_server_stats;
+
 int radik_server_create(const radik_server_config* cfg, radik_server** server);
 /* Queues one request (thread-safe, returns at once).  WITHSCALE / WITHIDXIN
  * requests are not served (RADIK_ENOTSUP). */
@@ -244,6 +271,8 @@ int radik_server_submit(radik_server* server, int dtype, uint32_t flags, const v
 int radik_server_poll(radik_server* server, radik_completion* out, int max, int* count);
 /* Blocks until every submitted request has finished; returns the first error. */
 int radik_server_drain(radik_server* server);
+/* Copies the server's batch counters into out. */
+int radik_server_get_stats(radik_server* server, radik_server_stats* out);
 /* Load generator: submits items at their arrival offsets from this host
  * thread (busy-waiting between them), drains, and writes each item's latency
  * (in item order) to latency_us.  No other thread may submit meanwhile. */

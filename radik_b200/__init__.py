@@ -71,6 +71,8 @@ def lib() -> ctypes.CDLL:
     L.radik_get_workspace_size_rows.argtypes = [i32, u32, i32, i64, i32, i32, ctypes.POINTER(sz)]
     L.radik_topk.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp]
     L.radik_topk_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp]
+    L.radik_topk_rows_ctas.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, i32, vp]
+    L.radik_engine_ctas.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.radik_get_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
     L.radik_autotune.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
                                  ctypes.POINTER(ctypes.c_int)]
@@ -93,6 +95,7 @@ def lib() -> ctypes.CDLL:
     L.radik_timeline_attach.restype = ctypes.c_int
     L.radik_version.argtypes = []
     for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
+                 "radik_topk_rows_ctas", "radik_engine_ctas",
                  "radik_get_status", "radik_version", "radik_topk_static", "radik_autotune_ex", "radik_autotune_rows",
                  "radik_autotune_save", "radik_autotune_load"):
         getattr(L, name).restype = ctypes.c_int
@@ -243,14 +246,27 @@ def topk(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bo
     return vals, idx
 
 
+def engine_ctas(device=None) -> int:
+    """Engine CTAs (one per SM) a call on ``device`` can use at most."""
+    import torch
+
+    out = ctypes.c_int(0)
+    with torch.cuda.device(device if device is not None else torch.cuda.current_device()):
+        _check(lib().radik_engine_ctas(ctypes.byref(out)))
+    return out.value
+
+
 def topk_rows(values, rows, *, largest: bool = True, sorted: bool = False, ascend: Optional[bool] = None,
               with_scale: bool = False, idx_in=None, idx64: bool = False, total_out: Optional[int] = None,
-              bounds: Optional[Tuple[int, int, int]] = None, workspace=None, stream=None, check: bool = True):
+              bounds: Optional[Tuple[int, int, int]] = None, workspace=None, stream=None, check: bool = True,
+              max_ctas: int = 0):
     """Uneven batched one-launch top-k.
 
     rows: host list of (in_off, out_off, n, k) or a device uint8/int64 tensor
     holding radik_row_desc records.  Returns flat (vals, idx) of total_out
     slots.  bounds = (total_n, n_max, k_max) for the workspace layout.
+    max_ctas > 0 runs the call on at most that many SMs
+    (radik_topk_rows_ctas), leaving the others to calls on other streams.
     """
     import torch
 
@@ -281,10 +297,11 @@ def topk_rows(values, rows, *, largest: bool = True, sorted: bool = False, ascen
                                     device=dev)
         vals = torch.empty(max(total_out, 1), dtype=values.dtype, device=dev)
         idx = torch.empty(max(total_out, 1), dtype=torch.int64 if idx64 else torch.int32, device=dev)
-        _check(lib().radik_topk_rows(dt, flags, values.data_ptr(), idx_in.data_ptr() if idx_in is not None else None,
-                                     vals.data_ptr(), idx.data_ptr(), workspace.data_ptr(), workspace.numel(),
-                                     desc.data_ptr(), B, int(total_n), int(n_max), int(k_max),
-                                     _stream_handle(stream, dev)))
+        _check(lib().radik_topk_rows_ctas(dt, flags, values.data_ptr(),
+                                          idx_in.data_ptr() if idx_in is not None else None, vals.data_ptr(),
+                                          idx.data_ptr(), workspace.data_ptr(), workspace.numel(), desc.data_ptr(), B,
+                                          int(total_n), int(n_max), int(k_max), int(max_ctas),
+                                          _stream_handle(stream, dev)))
     if check:
         status(workspace, stream)
     return vals[:total_out], idx[:total_out]
@@ -367,6 +384,12 @@ class Completion(ctypes.Structure):
                 ("latency_us", ctypes.c_double)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("batches", ctypes.c_int64), ("requests", ctypes.c_int64), ("batches_beside_others", ctypes.c_int64),
+                ("max_batches_in_flight", ctypes.c_int32), ("max_ctas_in_flight", ctypes.c_int32),
+                ("ctas_total", ctypes.c_int32), ("ctas_cap", ctypes.c_int32)]
+
+
 class TraceItem(ctypes.Structure):
     _fields_ = [("arrival_us", ctypes.c_double), ("dtype", ctypes.c_int), ("flags", ctypes.c_uint32),
                 ("values", ctypes.c_void_p), ("n", ctypes.c_int), ("k", ctypes.c_int),
@@ -384,8 +407,9 @@ def _server_lib():
         L.radik_server_drain.argtypes = [vp]
         L.radik_server_run_trace.argtypes = [vp, ctypes.POINTER(TraceItem), ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.radik_server_destroy.argtypes = [vp]
+        L.radik_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
         for name in ("radik_server_create", "radik_server_submit", "radik_server_poll", "radik_server_drain",
-                     "radik_server_run_trace", "radik_server_destroy"):
+                     "radik_server_run_trace", "radik_server_destroy", "radik_server_get_stats"):
             getattr(L, name).restype = ctypes.c_int
         L._server_bound = True
     return L
@@ -425,6 +449,12 @@ class Server:
 
     def drain(self) -> None:
         _check(self._L.radik_server_drain(self._h))
+
+    def stats(self) -> dict:
+        """The server's batch counters (radik_server_get_stats)."""
+        st = ServerStats()
+        _check(self._L.radik_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
 
     def run_trace(self, items) -> "list":
         """items: sequence of TraceItem; returns per-item latencies (us)."""

@@ -142,7 +142,7 @@ int env_int(const char* name, int dflt) {
 // chunks that the histogram items read two grids earlier, and that window
 // (2 x 148 x 128 KB) must stay in L2.  The 12-bit first digit (4096 bins,
 // 16 KB of smem) leaves about n/4096 keys of an i.i.d. row in the selected
-// bin.  Rows of up to 2^18 keys are selected by one CTA.  The autotuner
+// bin.  Rows of up to 2^15 keys are selected by one CTA.  The autotuner
 // (radik_autotune*) can replace each choice per shape bucket; RADIK_CH /
 // RADIK_CHR / RADIK_D1 / RADIK_CTA_CAP override everything (tuning sweeps).
 struct Config {
@@ -188,15 +188,17 @@ Tuned tuned_for(uint64_t bucket) {
   return it == g_tuned.end() ? Tuned{} : it->second;
 }
 
-// Rows of up to this many keys are selected by one CTA.  A call of few rows
-// (fewer than half the CTAs) leaves most of the grid idle that way, so there
-// only rows of up to 2^15 keys stay on one CTA and longer ones spread over
-// the grid (one 100K-key row: 97 us on one CTA's side team).
-int cta_cap_of(const Tuned& t, int B, int grid) {
+// Rows of up to this many keys are selected by one CTA (on its side team,
+// which streams them with plain loads); longer rows spread over the grid as
+// pre-filter rows.  Measured on a B200 with caps of 2^15 / 2^18:
+// 1024 x 2^17 keys, k = 256: 238 / 822 us; 512 x 2^18: 174 / 670 us;
+// 256 x 100000, k = 1000: 97 / 265 us; 2048 x 2^16, k = 32: 279 / 761 us;
+// 4096 uneven rows of n log-uniform in [2^10, 2^22]: 1.66 / 2.51 ms.
+int cta_cap_of(const Tuned& t) {
   const int ecap = env_int("RADIK_CTA_CAP", 0);
   if (ecap >= kCtaRowCapMin && ecap <= kCtaRowCapMax) return ecap;
   if (t.cta_cap) return t.cta_cap;
-  return B * 2 < grid ? kCtaRowCapMin : kCtaRowCap;
+  return kCtaRowCap;
 }
 
 // stream_elems: keys of the call's streamed rows; es: bytes per key; uniform_n:
@@ -229,7 +231,7 @@ Config choose_config(int64_t stream_elems, int grid, const Tuned& t, int es, int
   c.CH = t.ch ? t.ch : ch;
   c.CHR = 32768;
   c.D1 = t.d1 ? t.d1 : kMaxD1;
-  c.cta_cap = cta_cap_of(t, B, grid);
+  c.cta_cap = cta_cap_of(t);
   const int ech = env_int("RADIK_CH", 0);
   if (ech >= kMinCH && ech <= (1 << 24) && (ech % 16) == 0) c.CH = ech;
   const int echr = env_int("RADIK_CHR", 0);
@@ -349,7 +351,7 @@ int plan_call(int dtype, uint32_t flags, const int* task_len, int task_num, int 
   int grid = 0;
   int rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  const int cta_cap = cta_cap_of(t, B, grid);
+  const int cta_cap = cta_cap_of(t);
   int64_t multi_elems = 0;
   for (int i = 0; i < B; ++i) {
     const int kind = row_kind(task_len[i], K, cta_cap);
@@ -674,6 +676,14 @@ int radik_topk(int dtype, uint32_t flags, const void* val_in, const void* idx_in
 int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
                     void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
                     int task_num, int64_t total_n, int n_max, int k_max, void* stream_) {
+  return radik_topk_rows_ctas(dtype, flags, val_in, idx_in, val_out, idx_out, workspace, workspace_bytes, rows,
+                              task_num, total_n, n_max, k_max, 0, stream_);
+}
+
+int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
+                         void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
+                         int task_num, int64_t total_n, int n_max, int k_max, int max_ctas, void* stream_) {
+  if (max_ctas < 0) return fail(RADIK_EINVAL, "radik: negative max_ctas");
   int rc = check_common(dtype, flags, val_in, idx_in, val_out, idx_out, workspace);
   if (rc) return rc;
   if (task_num < 0 || total_n < 0 || n_max < 0 || k_max < 0) return fail(RADIK_EINVAL, "radik: negative size");
@@ -689,6 +699,9 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
+  // A smaller grid leaves SMs free for other work: every CTA of the engine
+  // stays resident (cooperative launch), whatever else runs beside it.
+  if (max_ctas > 0) grid = std::min(grid, max_ctas);
   const Config cfg = choose_config(total_n, grid, tuned_for(shape_bucket(dtype, flags, true, B, n_max, k_max)),
                                    (int)elem_bytes(dtype), 0, B);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
@@ -707,6 +720,11 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
   e = launch_engine(dtype, p, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "engine launch");
   return RADIK_OK;
+}
+
+int radik_engine_ctas(int* ctas) {
+  if (!ctas) return fail(RADIK_EINVAL, "radik: ctas is null");
+  return engine_grid(kF32, 0, ctas);
 }
 
 int radik_get_status(void* workspace, void* stream_, int* device_bits) {

@@ -38,7 +38,7 @@ constexpr int kCtasPerSM = 1;
 constexpr int kWarps = kThreads / 32;
 constexpr int kCapSB = 6144;             // candidates a finisher resolves in smem (48 KB)
 constexpr int kSmemRowCap = 8192;        // rows this short are selected in smem
-constexpr int kCtaRowCap = 1 << 18;      // default: rows this short are selected by one CTA
+constexpr int kCtaRowCap = 1 << 15;      // default: rows this short are selected by one CTA
 constexpr int kCtaRowCapMin = 1 << 15;   // range of the tunable one-CTA row cap
 constexpr int kCtaRowCapMax = 1 << 20;
 constexpr int kCapSort = 4096;           // outputs a finisher sorts in smem (32 KB)
@@ -46,6 +46,7 @@ constexpr int kMaxD1 = 12;               // widest first digit (16 KB smem hist)
 constexpr int kMinD1 = 8;
 constexpr int kPrefRatio = 64;           // pre-filter rows with k * 64 <= n
 constexpr int kSampleMax = 8192;         // sampled keys per row (32 KB smem)
+constexpr int kSampleStream = 16384;     // sampled keys of a streamed side-team sample (no smem)
 constexpr int kSampleMin = 1024;
 constexpr int kPhaseBSlots = 64;         // rows resolved together in phase B
 constexpr int kPhaseBChunk = 65536;      // phase-B chunk length (entries)

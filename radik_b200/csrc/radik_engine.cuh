@@ -65,7 +65,19 @@ enum TlSlot : int {
   kTlStart = 0, kTlFirstSample = 1, kTlConsDone = 2, kTlSideDone = 3, kTlFinEnd = 4, kTlPhaseB = 5, kTlEnd = 6,
   kTlFinStart = 7, kTlSampleIn = 8, kTlSampleIssue = 9, kTlSampleKeys = 10, kTlItemStart = 14, kTlChunkEnd = 15,
   kTlFinBegin = 16, kTlFinLoaded = 17,
-  kTlFinResolved = 18, kTlFinEmitted = 19, kTlFinPost = 20, kTlFinCands = 31
+  kTlFinResolved = 18, kTlFinEmitted = 19, kTlFinPost = 20, kTlFinCands = 31,
+  // per-CTA sums (SM clock cycles, or counts) of where the teams wait
+  kTlNChunks = 11, kTlNSide = 12, kTlNFin = 13,
+  kTlAccSideQ = 21,     // producer: blocked pushing to a full side queue
+  kTlAccConsQ = 22,     // producer: blocked pushing to a full consumer queue
+  kTlAccRing = 23,      // producer: waiting for a drained ring stage
+  kTlAccThr = 24,       // producer: waiting for a chunk's threshold
+  kTlAccFull = 25,      // consumer team: waiting for a stage's data
+  kTlAccPre = 26,       // consumer team: waiting for a threshold before a chunk
+  kTlAccConsIdle = 27,  // consumer team: waiting for an item
+  kTlAccFinWait = 28,   // a finish waiting for its row's chunks
+  kTlAccSideIdle = 29,  // side team: waiting for an item
+  kTlAccClaim = 30      // producer: claim round trips not hidden behind copies
 };
 #ifdef RADIK_TIMELINE
 __device__ __forceinline__ void tl_write(unsigned long long* tl, int slot, unsigned long long v) {
@@ -76,11 +88,21 @@ __device__ __forceinline__ unsigned long long tl_now() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+__device__ __forceinline__ void tl_add(unsigned long long* tl, int slot, unsigned long long v) {
+  if (tl) tl[(size_t)blockIdx.x * kTlSlots + slot] += v;
+}
 #define RADIK_TL(p, slot) tl_write((p).timeline, (slot), tl_now())
 #define RADIK_TL_VALUE(p, slot, v) tl_write((p).timeline, (slot), (unsigned long long)(v))
+// RADIK_TL_T0(t) starts a wait; RADIK_TL_ACC(p, slot, t) adds its cycles.
+#define RADIK_TL_T0(t) const long long t = clock64()
+#define RADIK_TL_ACC(p, slot, t) tl_add((p).timeline, (slot), (unsigned long long)(clock64() - (t)))
+#define RADIK_TL_COUNT(p, slot) tl_add((p).timeline, (slot), 1ull)
 #else
 #define RADIK_TL(p, slot) ((void)0)
 #define RADIK_TL_VALUE(p, slot, v) ((void)0)
+#define RADIK_TL_T0(t) ((void)0)
+#define RADIK_TL_ACC(p, slot, t) ((void)0)
+#define RADIK_TL_COUNT(p, slot) ((void)0)
 #endif
 
 // ----------------------------------------------------------------------------
@@ -272,7 +294,7 @@ static_assert(24 * (kSinkCand + kSinkOut) * 8 <= kConsAreaBytes, "filter staging
 static_assert(32 * (kSinkCand + kSinkOut) * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert((4 << kMaxD1) <= kConsAreaBytes, "histogram");
 static_assert(kResolveHistOff + 1024 <= kSideAreaBytes && 16384 <= kSideAreaBytes, "finisher area");
-static_assert(kSmemRowHistOff + 16384 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
+static_assert(kSmemRowHistOff + 1024 <= kSideAreaBytes && kCapSort * 8 <= kSideAreaBytes, "smem-row area");
 static_assert(32 * 128 * 8 <= kSideAreaBytes, "phase-B staging");
 static_assert(kSampleHistOff + 1024 <= kSideAreaBytes, "sample area");
 static_assert(kSampleRawOff + kSampleMax * 2 <= kSideAreaBytes, "16-bit sample staging");
@@ -1183,8 +1205,13 @@ struct Engine {
   template <typename PRE, typename FE, typename FV>
   __device__ void consume_chunk(const RowCtx& rc, const ItemDesc& d, PRE&& pre, FE&& fe, FV&& fv) {
     const char* row = static_cast<const char*>(p.val_in) + rc.in_off * ES;
+    RADIK_TL_T0(tp);
     pre();
-    if (ConsTeam::tid() == 0) RADIK_TL(p, kTlItemStart);
+    if (ConsTeam::tid() == 0) {
+      RADIK_TL_ACC(p, kTlAccPre, tp);
+      RADIK_TL_COUNT(p, kTlNChunks);
+      RADIK_TL(p, kTlItemStart);
+    }
     do_release();
     const int64_t head = d.va - d.a;
     const int64_t vb = d.va + d.nvec * VEC;
@@ -1210,12 +1237,14 @@ struct Engine {
     int64_t pos = d.va + (int64_t)ConsTeam::tid() * VEC;  // first element of this thread's vector in the stage
     for (int i = 0; i < d.nst; ++i) {
       uint32_t it = 0;
+      RADIK_TL_T0(tw);
       while (!mbar_try_wait(&ctl->full[slot], parity)) {
         if (++it > p.spin_limit) {
           if (ConsTeam::tid() == 0) atomicOr(&p.hdr->status, kStatusTimeout);
           break;
         }
       }
+      if (ConsTeam::tid() == 0) RADIK_TL_ACC(p, kTlAccFull, tw);
       const uint4* st = ring + slot * kStageVecs;
       if (i < nfull) {
 #pragma unroll
@@ -1279,10 +1308,53 @@ struct Engine {
       while (S < kSampleBig && (int64_t)S * 2 * 64 <= rc.n) S *= 2;
     }
     constexpr int SL = 128 / ES;  // keys per line
-    const int nlines = S / SL;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.val_in) + (uintptr_t)rc.in_off * ES;
     const int64_t first = (int64_t)((a + 127) / 128);
     const int64_t nfull = (int64_t)((a + (uintptr_t)rc.n * ES) / 128) - first;  // whole lines in the row
+    if (!big) {
+      // A larger sample streamed through registers.  When the threshold comes
+      // from per-thread minimums (small ranks), no sampled key is stored, so
+      // the sample is not bound by the team's area: up to n / 64 keys
+      // (kSampleStream).  For 2^20-key rows at k = 256 the threshold then
+      // passes about 1000 keys instead of 2500: fewer vectors take the
+      // consumers' exact test and the finish resolves fewer candidates.
+      int S2 = S;
+      while (S2 < kSampleStream && (int64_t)S2 * 2 * 64 <= rc.n) S2 *= 2;
+      const int r2 = sample_rank(rc.n, rc.k, S2);
+      if (S2 > S && r2 * 4 <= Tm::kSize) {
+        const int nv = S2 / SL * 8;  // 16-byte pieces of whole lines
+        const uint64_t step2 = ((uint64_t)(nfull - 1) << 32) / (uint64_t)(S2 / SL - 1);
+        uint32_t lo32 = 0xFFFFFFFFu, hi32 = 0;
+        constexpr int UL = 4;  // loads a thread keeps in flight
+        for (int b = Tm::tid(); b < nv; b += UL * Tm::kSize) {
+          uint4 v[UL];
+#pragma unroll
+          for (int u = 0; u < UL; ++u) {
+            const int j = b + u * Tm::kSize;
+            const int64_t line = first + (int64_t)(((uint64_t)(j >> 3) * step2) >> 32);
+            v[u] = j < nv ? ld_stream16(reinterpret_cast<const void*>((uintptr_t)line * 128 + (uintptr_t)(j & 7) * 16))
+                          : make_uint4(0, 0, 0, 0);
+          }
+#pragma unroll
+          for (int u = 0; u < UL; ++u) {
+            if (b + u * Tm::kSize < nv) {
+#pragma unroll
+              for (int e = 0; e < VEC; ++e) {
+                const uint32_t k = key_of(vec_elem<ES>(v[u], e), rc);
+                lo32 = min(lo32, k);
+                hi32 = max(hi32, k);
+              }
+            }
+          }
+        }
+        const uint64_t lo = lo32 == 0xFFFFFFFFu && hi32 == 0 ? ~0ull : (uint64_t)lo32, hi = hi32;
+        uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSampleHistOff);
+        const uint32_t t = block_sample_threshold<Tm, K::KB>(nullptr, S2, r2, lo, hi, hist, m, &p.hdr->status);
+        Tm::sync();
+        return t;
+      }
+    }
+    const int nlines = S / SL;
     // fp32 values are converted to keys in place; 16-bit values are staged apart
     uint8_t* raw = ES == 4 ? scratch : big ? scratch + S * 4 + 1024 : smem + kSampleRawOff;
     // line i sits at first + floor(i * (nfull - 1) / (nlines - 1)), stepped in
@@ -1351,7 +1423,10 @@ struct Engine {
     smem_resolve<Tm, VT, SCALE>(get, rc.n, rc, prefix, plen, krem, rc.n, reinterpret_cast<uint32_t*>(smem + kSmemRowHistOff), m,
                             &p.hdr->status);
     smem_emit<Tm, VT, SCALE>(p, get, rc.n, rc, prefix, plen, p.rs + r, m, true);
-    post_process<Tm, VT, SCALE>(p, rc, smem + kSmemRowHistOff, m);
+    // The outputs are written, so the row's values are dead: the sort takes
+    // the area from its base (up to kCapSort entries, 32 KB).  Behind the
+    // values it would run 14 KB past the side area into the control block.
+    post_process<Tm, VT, SCALE>(p, rc, smem, m);
   }
 
   // ---- one CTA, the whole row from global memory (n <= p.cta_cap)
@@ -1498,6 +1573,8 @@ struct Engine {
     if (Tm::tid() == 0) {
       const int32_t* t = &p.rs[r].fticket;
       uint32_t it = 0;
+      RADIK_TL_T0(tw);
+      RADIK_TL_COUNT(p, kTlNFin);
       while (ld_acquire(t) < rc.fin_wait) {
         if (++it > p.spin_limit) {
           atomicOr(&p.hdr->status, kStatusTimeout);
@@ -1505,6 +1582,7 @@ struct Engine {
         }
         __nanosleep(128);
       }
+      RADIK_TL_ACC(p, kTlAccFinWait, tw);
     }
     Tm::sync();
     if (Tm::tid() == 0) RADIK_TL(p, kTlFinStart);
@@ -1535,6 +1613,10 @@ struct Engine {
         T = d.thr;
         return;
       }
+      // The wait below may depend on this team's held-back chunk release
+      // (a finish waiting for that count can sit ahead of the threshold's
+      // sample on a side team), so the release goes first.
+      do_release();
       if (ConsTeam::tid() == 0 && m->t_row != r) {
         uint64_t v = ld_acquire_u64(&rs->tready);
         for (uint32_t it = 0; !(v >> 32); ++it) {
@@ -1682,6 +1764,7 @@ struct Engine {
     const uint32_t use = (uint32_t)(rc.slot_use / p.S);
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kHistOff);  // consumer area
     uint32_t* ghist = p.hist_ring + (size_t)s * ((size_t)1 << kMaxD1);
+    do_release();  // before a wait that a finish holding back the slot may need it for
     if (ConsTeam::tid() == 0) m->bcast = use == 0 ? 1 : (int)spin_until_ge(p.slot_gen + s, use);
     for (int i = ConsTeam::tid() * 4; i < NB; i += ConsTeam::kSize * 4) *reinterpret_cast<uint4*>(hist + i) = make_uint4(0, 0, 0, 0);
     ConsTeam::sync();
@@ -1753,6 +1836,7 @@ struct Engine {
   // ---- filter item of a radix row
   __device__ void f_item(int r, const RowCtx& rc, const ItemDesc& d) {
     RowState* rs = p.rs + r;
+    do_release();  // the bin wait below must not hold back another row's finish
     if (ConsTeam::tid() == 0) {
       int mode = kModeNone;
       if (spin_until_ge(reinterpret_cast<const uint32_t*>(&rs->ready), 1u)) mode = __ldcg(&rs->mode);
@@ -2336,12 +2420,14 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     if (i >= (uint32_t)kQ) {
       const uint32_t parity = ((i / kQ) - 1u) & 1u;
       uint32_t it = 0;
+      RADIK_TL_T0(tw);
       while (!mbar_try_wait(&empty[slot], parity)) {
         if (++it > p.spin_limit) {
           atomicOr(&p.hdr->status, kStatusTimeout);
           break;
         }
       }
+      RADIK_TL_ACC(p, full == ctl->sq_full ? kTlAccSideQ : kTlAccConsQ, tw);
     }
     slots[slot] = d;
     mbar_arrive(&full[slot]);
@@ -2405,11 +2491,13 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       // the wait ends.  A small call (early_copy) streams its few megabytes
       // while the thresholds are computed; its consumers wait for them.
       uint64_t v = ir.row == pf_row ? pf_tr : 0ull;
+      RADIK_TL_T0(tw);
       if (!(v >> 32)) v = ld_acquire_u64(&p.rs[ir.row].tready);
       for (uint32_t it = 0; !(v >> 32) && !p.early_copy && it < p.spin_limit; ++it) {
         __nanosleep(128);
         v = ld_acquire_u64(&p.rs[ir.row].tready);
       }
+      RADIK_TL_ACC(p, kTlAccThr, tw);
       d.thr = (uint32_t)v;
       d.thr_ok = (int32_t)(v >> 32);
     }
@@ -2453,12 +2541,14 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
       if (g >= NS) {
         const uint32_t parity = ((g / NS) - 1u) & 1u;
         uint32_t it = 0;
+        RADIK_TL_T0(tw);
         while (!mbar_try_wait(&ctl->empty[slot], parity)) {
           if (++it > p.spin_limit) {
             atomicOr(&p.hdr->status, kStatusTimeout);
             break;
           }
         }
+        RADIK_TL_ACC(p, kTlAccRing, tw);
       }
       const int64_t v0 = (int64_t)i * kStageVecs;
       const uint32_t bytes = stage_bytes(i);
@@ -2478,7 +2568,9 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     }
     if (late_claim && !last) {
       throttle(q);
+      RADIK_TL_T0(tw);
       nq = claim_item(p);
+      RADIK_TL_ACC(p, kTlAccClaim, tw);
     }
     q = nq;
   }
@@ -2578,8 +2670,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
         e.pending_rel = m->rel_row;
         if (e.pending_rel >= 0 && !mbar_try_wait(&ctl->cq_full[i % kQ], (i / kQ) & 1u)) e.do_release();
       }
+      RADIK_TL_T0(tw);
       const ItemDesc d = pop_item<ConsTeam>(ctl->cq_full, ctl->cq_empty, ctl->cq, i, p);
-      if (ConsTeam::tid() == 0) m->rel_row = -1;
+      if (ConsTeam::tid() == 0) {
+        RADIK_TL_ACC(p, kTlAccConsIdle, tw);
+        m->rel_row = -1;
+      }
       if (d.q < 0) break;
       const RowCtx rc = load_row<VT, SCALE>(p, d.row);
       if (d.fin) {
@@ -2607,7 +2703,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     // side team: samples, single-item rows, FIN items
     Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
     for (uint32_t i = 0;; ++i) {
+      RADIK_TL_T0(tw);
       const ItemDesc d = pop_item<SideTeam>(ctl->sq_full, ctl->sq_empty, ctl->sq, i, p);
+      if (SideTeam::tid() == 0) {
+        RADIK_TL_ACC(p, kTlAccSideIdle, tw);
+        RADIK_TL_COUNT(p, kTlNSide);
+      }
       if (d.q < 0) break;
       const RowCtx rc = load_row<VT, SCALE>(p, d.row);
       if (d.isA) {

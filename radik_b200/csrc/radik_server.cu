@@ -9,8 +9,14 @@
 // pointer, each row an element offset from it), scatters the results to the
 // requests' own buffers with one small kernel, and retires the batch when its
 // event completes.  Requests that arrive while batches run join the next
-// batch; several slots on their own streams keep batches in flight at once,
-// so admission, planning and copies overlap the selection kernels.
+// batch; several slots on their own streams keep batches in flight at once.
+//
+// SMs are the third resource a batch is admitted by, beside its slot and the
+// memory budget: the engine runs one CTA per SM, so a batch asks for one CTA
+// per 2^16 keys (at most three quarters of the device when several slots
+// exist) and starts only when that many SMs are free of other batches.  The
+// engines of concurrent batches therefore sit on disjoint SMs and run side by
+// side: a batch of small requests does not wait for a large one to finish.
 //
 // Per-request mode (radik_server_config::mode = 1) is the plain baseline: one
 // radik_topk launch per request, in arrival order on one stream.
@@ -85,8 +91,13 @@ struct Slot {
   int32_t* status_h = nullptr;  // pinned copy of the call's device status word
   std::vector<Req> reqs;
   size_t bytes = 0;
+  int ctas = 0;  // engine CTAs (SMs) the batch holds
   bool busy = false;
 };
+
+// Keys per engine CTA a batch asks for.  At 2^16 fp32 keys (256 KB) a CTA
+// streams its share in a few microseconds, about the engine's fixed cost.
+constexpr int64_t kKeysPerCta = (int64_t)1 << 16;
 
 }  // namespace
 
@@ -100,6 +111,10 @@ struct Server {
   std::atomic<uint64_t> next_id{1};
   std::atomic<int64_t> outstanding{0};
   size_t inflight_bytes = 0;
+  int ctas_total = 0;     // engine CTAs the device runs at once (one per SM)
+  int ctas_cap = 0;       // most CTAs one batch may take
+  int ctas_inflight = 0;  // CTAs held by batches in flight
+  radik_server_stats stats{};
   bool stop = false;
   std::thread worker;
   std::string error;
@@ -139,22 +154,37 @@ struct Server {
       }
       if (st != RADIK_OK && first_error == RADIK_OK) first_error = st;
       for (const Req& r : s.reqs) complete(r, st, t);
-      outstanding -= (int64_t)s.reqs.size();
-      inflight_bytes -= s.bytes;
-      s.reqs.clear();
-      s.bytes = 0;
-      s.busy = false;
-      cv.notify_all();
+      release(s);
     }
+  }
+
+  // Returns slot s's requests, bytes and SMs.  Caller holds mu.
+  void release(Slot& s) {
+    outstanding -= (int64_t)s.reqs.size();
+    inflight_bytes -= s.bytes;
+    ctas_inflight -= s.ctas;
+    s.reqs.clear();
+    s.bytes = 0;
+    s.ctas = 0;
+    s.busy = false;
+    cv.notify_all();
+  }
+
+  // Engine CTAs a batch of `keys` keys asks for.
+  int want_ctas(int64_t keys) const {
+    const int64_t w = (keys + kKeysPerCta - 1) / kKeysPerCta;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(w, ctas_cap));
   }
 
   // Takes one batch for slot s from the pending queue: the oldest request's
   // (dtype, flags) group, in arrival order, within the slot's row, key and
-  // output limits and the memory budget; reserves the slot.  Caller holds mu.
+  // output limits, the memory budget and the free SMs; reserves the slot and
+  // the batch's SMs.  Caller holds mu.
   bool form(Slot& s) {
     if (pending.empty()) return false;
     const int dtype = pending.front().dtype;
     const uint32_t flags = pending.front().flags;
+    const int free_ctas = ctas_total - ctas_inflight;
     int64_t keys = 0, outs = 0;
     size_t bytes = 0;
     s.reqs.clear();
@@ -167,8 +197,9 @@ struct Server {
       const size_t b = req_bytes(*it);
       if (s.reqs.empty()) {
         if (inflight_bytes > 0 && inflight_bytes + b > cfg.budget_bytes) return false;  // wait for memory
+        if (want_ctas(it->n) > free_ctas) return false;                                 // wait for SMs
       } else if (keys + it->n > cfg.max_batch_keys || outs + it->k > (int64_t)cfg.max_batch_rows * cfg.max_k ||
-                 inflight_bytes + bytes + b > cfg.budget_bytes) {
+                 inflight_bytes + bytes + b > cfg.budget_bytes || want_ctas(keys + it->n) > free_ctas) {
         break;
       }
       s.reqs.push_back(*it);
@@ -179,8 +210,10 @@ struct Server {
     }
     if (s.reqs.empty()) return false;
     s.bytes = bytes;
+    s.ctas = want_ctas(keys);
     s.busy = true;
     inflight_bytes += bytes;
+    ctas_inflight += s.ctas;
     return true;
   }
 
@@ -226,8 +259,8 @@ struct Server {
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(s.sc_d, s.sc_h, sizeof(ScatterDesc) * B, cudaMemcpyHostToDevice, s.stream);
       if (e != cudaSuccess) return RADIK_ECUDA;
-      rc = radik_topk_rows(dtype, flags, reinterpret_cast<const void*>(base), nullptr, s.vout, s.iout, s.ws, s.ws_bytes,
-                           s.desc_d, B, keys, n_max, k_max, s.stream);
+      rc = radik_topk_rows_ctas(dtype, flags, reinterpret_cast<const void*>(base), nullptr, s.vout, s.iout, s.ws,
+                                s.ws_bytes, s.desc_d, B, keys, n_max, k_max, s.ctas, s.stream);
       if (rc == RADIK_OK) {
         scatter_kernel<<<B, 128, 0, s.stream>>>(s.sc_d, s.vout, s.iout, es, is);
         e = cudaGetLastError();
@@ -255,8 +288,10 @@ struct Server {
             s.reqs.assign(1, pending.front());
             pending.pop_front();
             s.bytes = req_bytes(s.reqs[0]);
+            s.ctas = ctas_total;
             s.busy = true;
             inflight_bytes += s.bytes;
+            ctas_inflight += s.ctas;
             ready = &s;
           } else if (form(s)) {
             ready = &s;
@@ -265,6 +300,13 @@ struct Server {
         if (ready) break;
       }
       if (ready) {
+        int others = 0;
+        for (const Slot& o : slots) others += (o.busy && &o != ready) ? 1 : 0;
+        ++stats.batches;
+        stats.requests += (int64_t)ready->reqs.size();
+        if (others > 0) ++stats.batches_beside_others;
+        stats.max_batches_in_flight = std::max(stats.max_batches_in_flight, others + 1);
+        stats.max_ctas_in_flight = std::max(stats.max_ctas_in_flight, ctas_inflight);
         lock.unlock();
         const int rc = issue(*ready);
         lock.lock();
@@ -273,12 +315,7 @@ struct Server {
           error = std::string("radik_server: launch failed: ") + radik_last_error();
           const double t = now_us();
           for (const Req& r : ready->reqs) complete(r, rc, t);
-          outstanding -= (int64_t)ready->reqs.size();
-          inflight_bytes -= ready->bytes;
-          ready->reqs.clear();
-          ready->bytes = 0;
-          ready->busy = false;
-          cv.notify_all();
+          release(*ready);
         }
         continue;
       }
@@ -322,9 +359,13 @@ int radik_server_create(const radik_server_config* cfg_in, radik_server** out) {
   if (cfg.max_n > cfg.max_batch_keys) cfg.max_batch_keys = cfg.max_n;
   cudaError_t e = cudaSetDevice(cfg.device);
   if (e != cudaSuccess) return RADIK_ECUDA;
+  int ctas = 0;
+  if (radik_engine_ctas(&ctas) != RADIK_OK || ctas <= 0) return RADIK_ECUDA;
   auto* h = new radik_server();
   Server& S = h->s;
   S.cfg = cfg;
+  S.ctas_total = ctas;
+  S.ctas_cap = cfg.slots > 1 ? std::max(1, ctas * 3 / 4) : ctas;
   S.slots.resize(cfg.slots);
   const uint32_t all = kFlagSorted | kFlagLargest | kFlagIdx64;
   for (Slot& sl : S.slots) {
@@ -392,6 +433,16 @@ int radik_server_poll(radik_server* h, radik_completion* out, int max, int* coun
   if (out && c > 0) std::copy(S.completed.begin(), S.completed.begin() + c, out);
   S.completed.erase(S.completed.begin(), S.completed.begin() + c);
   *count = c;
+  return RADIK_OK;
+}
+
+int radik_server_get_stats(radik_server* h, radik_server_stats* out) {
+  if (!h || !out) return RADIK_EINVAL;
+  Server& S = h->s;
+  std::lock_guard<std::mutex> lock(S.mu);
+  *out = S.stats;
+  out->ctas_total = S.ctas_total;
+  out->ctas_cap = S.ctas_cap;
   return RADIK_OK;
 }
 

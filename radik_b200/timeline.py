@@ -47,6 +47,10 @@ PHASES = {0: "start", 9: "sample_issue", 8: "sample_in", 10: "sample_keys", 1: "
           3: "side_done", 7: "fin_start", 16: "fin_begin", 17: "fin_loaded", 18: "fin_resolved",
           19: "fin_emitted", 20: "fin_post", 4: "fin_end", 5: "phase_b", 6: "end"}
 CANDS_SLOT = 31
+# per-CTA sums of wait cycles (SM clock) and item counts
+WAITS = {21: "prod_side_queue", 22: "prod_cons_queue", 23: "prod_ring", 24: "prod_threshold", 30: "prod_claim",
+         25: "cons_stage_data", 26: "cons_threshold", 27: "cons_idle", 28: "fin_wait_chunks", 29: "side_idle"}
+COUNTS = {11: "chunk_items", 12: "side_items", 13: "finishes"}
 DEFAULT_SHAPES = ("f32:1:1048576:256", "f32:1:16777216:256", "f32:1:16777216:4096", "f32:16:1048576:256",
                   "f32:256:1048576:256", "f16:256:1048576:256", "f32:1:1000:10", "f32:1:100000:256")
 
@@ -133,9 +137,17 @@ def measure(shape: str, flush_bytes: int = 256 << 20) -> dict:
         col = (col[col > 0] - t0).astype(np.float64) / 1e3
         if col.size:
             phases[name] = [round(float(col.min()), 2), round(float(np.median(col)), 2), round(float(col.max()), 2)]
+    mhz = 1965.0  # the B200's maximum SM clock, which an unthrottled run holds
+    waits = {}
+    for slot, name in WAITS.items():
+        col = t[:, slot].astype(np.float64) / mhz
+        waits[name] = [round(float(col.min()), 2), round(float(np.median(col)), 2), round(float(col.max()), 2)]
+    counts = {name: [int(t[:, slot].min()), float(np.median(t[:, slot])), int(t[:, slot].max())]
+              for slot, name in COUNTS.items()}
     return {"shape": {"dtype": dt, "rows": B, "n": n, "k": k}, "ctas": int(ran.sum()),
             "graph_us_per_call": round(graph_us, 2), "finish_candidates_max": int(cands.max()),
-            "phases_us_min_median_max": phases}
+            "phases_us_min_median_max": phases, "waits_us_per_cta_min_median_max": waits,
+            "counts_per_cta_min_median_max": counts}
 
 
 def main(argv=None) -> int:
@@ -153,6 +165,10 @@ def main(argv=None) -> int:
               f"(graph), finish candidates {r['finish_candidates_max']}", flush=True)
         for name, (lo, med, hi) in sorted(r["phases_us_min_median_max"].items(), key=lambda kv: kv[1][1]):
             print(f"    {name:13s} {lo:9.2f} {med:9.2f} {hi:9.2f}")
+        print("    waits per CTA (us at the SM clock), min / median / max:")
+        for name, (lo, med, hi) in r["waits_us_per_cta_min_median_max"].items():
+            print(f"      {name:16s} {lo:9.2f} {med:9.2f} {hi:9.2f}")
+        print("    items per CTA:", r["counts_per_cta_min_median_max"])
     return 0
 
 

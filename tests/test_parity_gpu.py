@@ -103,6 +103,17 @@ def test_parity_uneven_rows_and_idle_fill():
         assert_same_selection(got, want, lengths, [k] * len(lengths), [r * k for r in range(len(lengths))], sorted_)
 
 
+@pytest.mark.parametrize("k", [2049, 4096, 5000, 8192])
+def test_sorted_short_rows_with_large_k(k):
+    # rows held in shared memory (n <= 8192) whose sorted outputs exceed
+    # 2048 entries: the sort's scratch must stay inside the team's area
+    lengths = [5000, 8192, 2500, 8000]
+    flat = np.concatenate([values_for(rk.F32, n, "normal", 60 + r) for r, n in enumerate(lengths)])
+    for largest in (True, False):
+        got, want = run_both(flat, lengths, k, rk.F32, largest, True)
+        assert_same_selection(got, want, lengths, [k] * len(lengths), [r * k for r in range(len(lengths))], True)
+
+
 @pytest.mark.parametrize("dtype", [rk.F32, rk.F16])
 def test_parity_withscale(dtype):
     g = workloads.rng(2)

@@ -744,66 +744,91 @@ def side_by_side(dev, reps=20):
     """Two batches of the serving mix on two streams, as the server runs them:
     A = one 2^24-key fp32 request (k = 1024) on three quarters of the SMs,
     B = 16 requests of 32000 keys (k = 50) on the rest
-    (radik_topk_rows_ctas).  Times each alone and both launched together (CUDA
-    events from one origin event; medians of `reps`).  Together about equal
-    to the longer one alone means the two selections ran at the same time;
-    B's completion beside A shows a small batch not waiting for a large one.
-    Both outputs are checked against the oracle."""
+    (radik_topk_rows_ctas; buffers allocated up front, launches through the C
+    ABI).  Each rep holds both streams behind a short device-side delay so
+    the host has enqueued both calls before the GPU starts them; then each
+    call's device span (radik_get_call_span: the GPU global timer when its
+    selection kernel's first CTA started and its last CTA ended) shows
+    whether the two kernels ran at the same time.  Reported: medians over
+    the reps of each call's span alone and side by side, and of the time both
+    kernels were running at once.  Both outputs are checked against the
+    oracle."""
     import torch
 
     import oracle
     import radik_b200 as rk
     from radik_b200 import workloads
 
+    L = rk.lib()
     total = rk.engine_ctas(dev.index)
     a_ctas = total * 3 // 4
     b_ctas = total - a_ctas
+    flags = rk.make_flags(True, False)
     xa = workloads.normal(1 << 24, 61)
     xb = workloads.normal(16 * 32000, 62)
-    ta, tb = torch.from_numpy(xa).to(dev), torch.from_numpy(xb).to(dev)
-    rows_a = [(0, 0, 1 << 24, 1024)]
-    rows_b = [(j * 32000, j * 50, 32000, 50) for j in range(16)]
-    sa, sb = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    calls = {}
+    for name, x, rows, ctas in (("a", xa, [(0, 0, 1 << 24, 1024)], a_ctas),
+                                ("b", xb, [(j * 32000, j * 50, 32000, 50) for j in range(16)], b_ctas)):
+        desc = np.zeros(len(rows), dtype=[("in_off", "<i8"), ("out_off", "<i8"), ("n", "<i4"), ("k", "<i4")])
+        for r, (a, o, n, k) in enumerate(rows):
+            desc[r] = (a, o, n, k)
+        total_n, n_max, k_max = sum(r[2] for r in rows), max(r[2] for r in rows), max(r[3] for r in rows)
+        out_n = sum(r[3] for r in rows)
+        calls[name] = {
+            "x": x, "rows": rows, "ctas": ctas, "bounds": (total_n, n_max, k_max),
+            "vals_in": torch.from_numpy(x).to(dev),
+            "desc": torch.from_numpy(desc.view(np.uint8).copy()).to(dev),
+            "ws": torch.empty(rk.get_rows_workspace_size(rk.F32, len(rows), total_n, n_max, k_max, flags),
+                              dtype=torch.uint8, device=dev),
+            "vals": torch.empty(out_n, dtype=torch.float32, device=dev),
+            "idx": torch.empty(out_n, dtype=torch.int32, device=dev),
+            "stream": torch.cuda.Stream(dev)}
+
+    def launch(c):
+        total_n, n_max, k_max = c["bounds"]
+        rk._check(L.radik_topk_rows_ctas(rk.F32, flags, c["vals_in"].data_ptr(), None, c["vals"].data_ptr(),
+                                         c["idx"].data_ptr(), c["ws"].data_ptr(), c["ws"].numel(),
+                                         c["desc"].data_ptr(), len(c["rows"]), total_n, n_max, k_max, c["ctas"],
+                                         c["stream"].cuda_stream))
+
+    def rep(which):
+        for name in which:
+            with torch.cuda.stream(calls[name]["stream"]):
+                torch.cuda._sleep(200_000)
+        for name in which:
+            launch(calls[name])
+        spans = {name: rk.call_span(calls[name]["ws"], calls[name]["stream"]) for name in which}
+        for name in which:
+            rk.status(calls[name]["ws"], calls[name]["stream"])
+        return spans
+
     res = {}
-
-    def run(which):
-        e0 = torch.cuda.Event(enable_timing=True)
-        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(sa)
-        sb.wait_event(e0)
-        out = {}
-        if "a" in which:
-            out["a"] = rk.topk_rows(ta, rows_a, max_ctas=a_ctas, stream=sa, check=False)
-        if "b" in which:
-            out["b"] = rk.topk_rows(tb, rows_b, max_ctas=b_ctas, stream=sb, check=False)
-        ea.record(sa)
-        eb.record(sb)
-        return e0, ea, eb, out
-
     for which in ("a", "b", "ab"):
         for _ in range(3):
-            run(which)
-        torch.cuda.synchronize(dev)
-        marks = [run(which) for _ in range(reps)]
-        torch.cuda.synchronize(dev)
-        ta_us = [e0.elapsed_time(ea) * 1e3 for e0, ea, _, _ in marks]
-        tb_us = [e0.elapsed_time(eb) * 1e3 for e0, _, eb, _ in marks]
-        if which == "a":
-            res["a_alone_us"] = round(statistics.median(ta_us), 1)
-        elif which == "b":
-            res["b_alone_us"] = round(statistics.median(tb_us), 1)
-        else:
-            res["together_us"] = round(statistics.median([max(x, y) for x, y in zip(ta_us, tb_us)]), 1)
-            res["b_done_beside_a_us"] = round(statistics.median(tb_us), 1)
-            last = marks[-1][3]
+            rep(which)
+        runs = [rep(which) for _ in range(reps)]
+        for name in which:
+            key = f"{name}_{'alone' if len(which) == 1 else 'beside'}_us"
+            res[key] = round(statistics.median([(r[name][1] - r[name][0]) / 1e3 for r in runs]), 1)
+        if which == "ab":
+            both = [max(0, min(r["a"][1], r["b"][1]) - max(r["a"][0], r["b"][0])) / 1e3 for r in runs]
+            first = [min(r["a"][0], r["b"][0]) for r in runs]
+            res["both_running_us"] = round(statistics.median(both), 1)
+            res["together_us"] = round(statistics.median([(max(r["a"][1], r["b"][1]) - f) / 1e3
+                                                          for r, f in zip(runs, first)]), 1)
+            last = runs[-1]
+            t0 = min(last["a"][0], last["b"][0])
+            res["last_rep_spans_us"] = {n: [round((last[n][0] - t0) / 1e3, 1), round((last[n][1] - t0) / 1e3, 1)]
+                                        for n in ("a", "b")}
     res["serial_sum_us"] = round(res["a_alone_us"] + res["b_alone_us"], 1)
     res["overlap_ratio"] = round(res["serial_sum_us"] / max(res["together_us"], 1e-9), 3)
     res["ctas"] = {"a": a_ctas, "b": b_ctas, "device": total}
     bad = 0
-    for x, rows, got in ((xa, rows_a, last["a"]), (xb, rows_b, last["b"])):
+    for c in calls.values():
+        rows = c["rows"]
         ns, ks, oo = [r[2] for r in rows], [r[3] for r in rows], [r[1] for r in rows]
-        ov, oi = oracle.topk(x, ns, ks, flags=oracle.flags_of(True, False), out_offsets=oo)
-        gv, gi = _bits(got[0].cpu().numpy()), got[1].cpu().numpy().astype(np.int64)
+        ov, oi = oracle.topk(c["x"], ns, ks, flags=oracle.flags_of(True, False), out_offsets=oo)
+        gv, gi = _bits(c["vals"].cpu().numpy()), c["idx"].cpu().numpy().astype(np.int64)
         ov = _bits(ov)
         for n, k, o in zip(ns, ks, oo):
             a = np.argsort(gi[o:o + k], kind="stable")
@@ -811,9 +836,10 @@ def side_by_side(dev, reps=20):
             if not (np.array_equal(gi[o:o + k][a], oi[o:o + k][b].astype(np.int64))
                     and np.array_equal(gv[o:o + k][a], ov[o:o + k][b])):
                 bad += 1
-    res["parity"] = {"rows": len(rows_a) + len(rows_b), "exact": bad == 0, "mismatched_rows": bad}
-    res["note"] = ("A: one 2^24-key fp32 row, k=1024, on %d CTAs; B: 16 rows of 32000, k=50, on %d CTAs; "
-                   "overlap_ratio = (A alone + B alone) / together" % (a_ctas, b_ctas))
+    res["parity"] = {"rows": 17, "exact": bad == 0, "mismatched_rows": bad}
+    res["note"] = ("A: one 2^24-key fp32 row, k=1024, on %d CTAs; B: 16 rows of 32000, k=50, on %d CTAs; spans are "
+                   "the selection kernels' device spans (GPU global timer); both_running_us = time both kernels "
+                   "ran at once; overlap_ratio = (A alone + B alone) / together" % (a_ctas, b_ctas))
     return res
 
 

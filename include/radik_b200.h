@@ -93,10 +93,14 @@ int radik_topk_rows(int dtype, uint32_t flags, const void* val_in, const void* i
                     int task_num, int64_t total_n, int n_max, int k_max, void* stream);
 
 /* radik_topk_rows on at most max_ctas SMs (0: the whole device; the engine
- * runs one CTA per SM).  Calls on different streams whose grids add up to at
- * most the SM count run side by side on the device; the serving loop sizes
- * its batches this way.  No RadiK counterpart: RadiK sizes its grid from the
- * shape alone (topk_radixselect.h:117-130). */
+ * runs one CTA per SM).  Below the whole device the launch is not cooperative,
+ * so calls on other streams run side by side with it.  The engine's CTAs wait
+ * for one another, so the caller keeps the max_ctas of the calls in flight at
+ * once within radik_engine_ctas(): a CTA that finds no free SM delays its
+ * call, and one that never finds one makes the call's waits give up
+ * (RADIK_ETIMEOUT from radik_get_status).  The serving loop sizes its batches
+ * this way.  No RadiK counterpart: RadiK sizes its grid from the shape alone
+ * (topk_radixselect.h:117-130). */
 int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const void* idx_in, void* val_out,
                          void* idx_out, void* workspace, size_t workspace_bytes, const radik_row_desc* rows,
                          int task_num, int64_t total_n, int n_max, int k_max, int max_ctas, void* stream);
@@ -104,6 +108,13 @@ int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const vo
 /* Engine CTAs a call on the current device can use at most (one per SM):
  * the limit that radik_topk_rows_ctas calls share. */
 int radik_engine_ctas(int* ctas);
+
+/* Synchronises the stream and reads when the last call made with this
+ * workspace ran on the device: the GPU global timer (ns) at which its
+ * selection kernel's first CTA started and its last CTA ended (0 if the
+ * kernel did not run).  Spans of calls on different streams share one time
+ * base, so they show whether the calls ran at the same time. */
+int radik_get_call_span(void* workspace, void* stream, uint64_t* start_ns, uint64_t* end_ns);
 
 /* Synchronises the stream and returns the status of the last call made with
  * this workspace (RADIK_OK, RADIK_ETIMEOUT, RADIK_EINTERNAL, RADIK_EWORKSPACE).

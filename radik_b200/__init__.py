@@ -73,6 +73,7 @@ def lib() -> ctypes.CDLL:
     L.radik_topk_rows.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, vp]
     L.radik_topk_rows_ctas.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, vp, i32, i64, i32, i32, i32, vp]
     L.radik_engine_ctas.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.radik_get_call_span.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.radik_get_status.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
     L.radik_autotune.argtypes = [i32, u32, vp, vp, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_int), i32, i32, vp,
                                  ctypes.POINTER(ctypes.c_int)]
@@ -95,7 +96,7 @@ def lib() -> ctypes.CDLL:
     L.radik_timeline_attach.restype = ctypes.c_int
     L.radik_version.argtypes = []
     for name in ("radik_get_workspace_size", "radik_get_workspace_size_rows", "radik_topk", "radik_topk_rows",
-                 "radik_topk_rows_ctas", "radik_engine_ctas",
+                 "radik_topk_rows_ctas", "radik_engine_ctas", "radik_get_call_span",
                  "radik_get_status", "radik_version", "radik_topk_static", "radik_autotune_ex", "radik_autotune_rows",
                  "radik_autotune_save", "radik_autotune_load"):
         getattr(L, name).restype = ctypes.c_int
@@ -205,6 +206,17 @@ def status(workspace, stream=None) -> int:
         _check(lib().radik_get_status(workspace.data_ptr(), _stream_handle(stream, workspace.device),
                                       ctypes.byref(bits)))
     return bits.value
+
+
+def call_span(workspace, stream=None) -> Tuple[int, int]:
+    """(start_ns, end_ns): the GPU global-timer span of the selection kernel
+    of the last call made with ``workspace`` (radik_get_call_span).
+    Synchronises ``stream``."""
+    t0, t1 = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    with _device_of(workspace):
+        _check(lib().radik_get_call_span(workspace.data_ptr(), _stream_handle(stream, workspace.device),
+                                         ctypes.byref(t0), ctypes.byref(t1)))
+    return t0.value, t1.value
 
 
 def topk(values, k: int, lengths: Optional[Sequence[int]] = None, *, largest: bool = True, sorted: bool = False,

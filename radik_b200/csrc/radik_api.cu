@@ -21,7 +21,7 @@
 
 namespace radik {
 
-cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream, bool coop = true);
 cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int cta_cap, int D, uint32_t flags,
                         RowPlan* plans, int32_t* a_row, int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap,
                         int64_t cand_cap_total, int64_t sort_cap_total, int grid, cudaStream_t stream);
@@ -699,8 +699,11 @@ int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const vo
   int grid = 0;
   rc = engine_grid(dtype, flags, &grid);
   if (rc) return rc;
-  // A smaller grid leaves SMs free for other work: every CTA of the engine
-  // stays resident (cooperative launch), whatever else runs beside it.
+  // A smaller grid leaves SMs free for other work.  Its launch is not
+  // cooperative, so that launches on other streams can run beside it; its
+  // CTAs are all resident as long as the grids of the calls in flight add up
+  // to at most the SM count (the contract of this entry point).
+  const bool coop = !(max_ctas > 0 && max_ctas < grid);
   if (max_ctas > 0) grid = std::min(grid, max_ctas);
   const Config cfg = choose_config(total_n, grid, tuned_for(shape_bucket(dtype, flags, true, B, n_max, k_max)),
                                    (int)elem_bytes(dtype), 0, B);
@@ -717,8 +720,20 @@ int radik_topk_rows_ctas(int dtype, uint32_t flags, const void* val_in, const vo
                   reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, b.na, b.nb,
                   b.cand, b.sort, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan launch");
-  e = launch_engine(dtype, p, grid, stream);
+  e = launch_engine(dtype, p, grid, stream, coop);
   if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+  return RADIK_OK;
+}
+
+int radik_get_call_span(void* workspace, void* stream_, uint64_t* start_ns, uint64_t* end_ns) {
+  if (!workspace) return fail(RADIK_EWORKSPACE, "radik: workspace should not be null");
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream_));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+  uint64_t t[2] = {0, 0};
+  e = cudaMemcpy(t, static_cast<uint8_t*>(workspace) + offsetof(Header, t_first), sizeof(t), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy span");
+  if (start_ns) *start_ns = t[0];
+  if (end_ns) *end_ns = t[1];
   return RADIK_OK;
 }
 

@@ -2595,11 +2595,22 @@ __device__ __forceinline__ ItemDesc pop_item(uint64_t* full, uint64_t* empty, co
   return d;
 }
 
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 template <int VT, bool SCALE>
 __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __grid_constant__ EngineParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
   Ctrl* ctl = ctrl_of(smem);
-  if (threadIdx.x == 0) RADIK_TL(p, kTlStart);
+  if (threadIdx.x == 0) {
+    RADIK_TL(p, kTlStart);
+    // the call's device span (radik_get_call_span): the first CTA to start
+    // sets the start, every CTA raises the end as it leaves
+    atomicCAS(reinterpret_cast<unsigned long long*>(&p.hdr->t_first), 0ull, globaltimer_ns());
+  }
   if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
   if (threadIdx.x == 0) {
     for (int i = 0; i < ring_stages<VT>(); ++i) {
@@ -2731,13 +2742,20 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   // phase B: the whole CTA, scratch in the side area
   Engine<VT, SCALE> e(p, smem, smem + kSideAreaOff, side_misc(smem));
   e.phase_b();
-  if (threadIdx.x == 0) RADIK_TL(p, kTlEnd);
+  if (threadIdx.x == 0) {
+    RADIK_TL(p, kTlEnd);
+    atomicMax(reinterpret_cast<unsigned long long*>(&p.hdr->t_last), globaltimer_ns());
+  }
 }
 
 }  // namespace dev
 
+// coop = false launches the same grid without the cooperative attribute: for
+// a grid below the device's, whose caller keeps the grids of concurrent
+// launches within the SM count (every CTA then finds a free SM); cooperative
+// launches of the engine did not run side by side on a B200.
 template <int VT, bool SCALE>
-inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t stream) {
+inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t stream, bool coop = true) {
   auto kern = dev::engine_kernel<VT, SCALE>;
   // The smem opt-in is per device; remember which devices have it.  Callers
   // on several host threads (a serving worker beside the application) may
@@ -2766,7 +2784,7 @@ inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t st
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = coop ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, p);
 }
 
@@ -2780,9 +2798,9 @@ inline cudaError_t engine_occupancy(int* per_sm) {
 }
 
 // Per value type entry points (one translation unit each).
-cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream);
-cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream);
-cudaError_t launch_engine_bf16(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
+cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
+cudaError_t launch_engine_bf16(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
 cudaError_t occupancy_f32(uint32_t flags, int* per_sm);
 cudaError_t occupancy_f16(uint32_t flags, int* per_sm);
 cudaError_t occupancy_bf16(uint32_t flags, int* per_sm);

@@ -4,9 +4,9 @@
 
 namespace radik {
 
-cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream) {
-  return (p.flags & kFlagWithScale) ? launch_typed<kF16, true>(p, grid, stream)
-                                    : launch_typed<kF16, false>(p, grid, stream);
+cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream, bool coop) {
+  return (p.flags & kFlagWithScale) ? launch_typed<kF16, true>(p, grid, stream, coop)
+                                    : launch_typed<kF16, false>(p, grid, stream, coop);
 }
 
 cudaError_t occupancy_f16(uint32_t flags, int* per_sm) {

@@ -4,9 +4,9 @@
 
 namespace radik {
 
-cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream) {
-  return (p.flags & kFlagWithScale) ? launch_typed<kF32, true>(p, grid, stream)
-                                    : launch_typed<kF32, false>(p, grid, stream);
+cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream, bool coop) {
+  return (p.flags & kFlagWithScale) ? launch_typed<kF32, true>(p, grid, stream, coop)
+                                    : launch_typed<kF32, false>(p, grid, stream, coop);
 }
 
 cudaError_t occupancy_f32(uint32_t flags, int* per_sm) {

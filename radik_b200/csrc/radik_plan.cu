@@ -161,11 +161,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 }  // namespace dev
 
-cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream) {
+cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream, bool coop) {
   switch (dtype) {
-    case kF32: return launch_engine_f32(p, grid, stream);
-    case kF16: return launch_engine_f16(p, grid, stream);
-    case kBF16: return launch_engine_bf16(p, grid, stream);
+    case kF32: return launch_engine_f32(p, grid, stream, coop);
+    case kF16: return launch_engine_f16(p, grid, stream, coop);
+    case kBF16: return launch_engine_bf16(p, grid, stream, coop);
     default: return cudaErrorInvalidValue;
   }
 }

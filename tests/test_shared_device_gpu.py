@@ -1,8 +1,8 @@
 """radik_topk_rows_ctas: the rows form on part of the device.
 
-The engine is one cooperative launch of one CTA per SM; with max_ctas it
-takes fewer SMs, so calls on other streams can run beside it (the serving
-loop admits batches this way).  Every grid size must select exactly as the
+The engine runs one CTA per SM; with max_ctas it takes fewer SMs, in a
+launch that is not cooperative, so calls on other streams can run beside it
+(the serving loop admits batches this way).  Every grid size must select exactly as the
 whole device does: each case is checked against the CPU oracle, including
 grids of one and a few CTAs, radix rows, rows that fall back to the grid-wide
 tail (all keys tied) and two calls in flight at once on disjoint SMs."""
@@ -77,8 +77,13 @@ def test_two_calls_side_by_side_on_disjoint_sms():
     sa, sb = torch.cuda.Stream(DEV), torch.cuda.Stream(DEV)
     torch.cuda.synchronize()
     for _ in range(3):
-        ga = rk.topk_rows(ta, rows_a, max_ctas=a_ctas, stream=sa, check=False)
-        gb = rk.topk_rows(tb, rows_b, max_ctas=b_ctas, stream=sb, check=False)
+        # each call's descriptors, workspace and outputs are allocated on its
+        # own stream, so the caching allocator never hands one call's memory
+        # to the other while it runs
+        with torch.cuda.stream(sa):
+            ga = rk.topk_rows(ta, rows_a, max_ctas=a_ctas, check=False)
+        with torch.cuda.stream(sb):
+            gb = rk.topk_rows(tb, rows_b, max_ctas=b_ctas, check=False)
         torch.cuda.synchronize()
         _check(xa, rows_a, oo_a, ga, False, "side by side, large batch")
         _check(xb, rows_b, oo_b, gb, False, "side by side, small batch")
@@ -114,3 +119,15 @@ def test_server_runs_batches_beside_each_other():
         want = oracle.topk(xh, [xh.size], v.numel(), flags=oracle.flags_of(True, False))
         assert_same_selection((v.cpu().numpy(), i.cpu().numpy()), want, [xh.size], [v.numel()], [0], False,
                               f"request {j}")
+
+
+def test_call_span_is_recorded():
+    x, rows, oo = _rows_case([1 << 20, 40000], [256, 64], 7)
+    t = torch.from_numpy(x).to(DEV)
+    flags = rk.make_flags(True, False)
+    ws = torch.empty(rk.get_rows_workspace_size(rk.F32, len(rows), sum(r[2] for r in rows), 1 << 20, 256, flags),
+                     dtype=torch.uint8, device=DEV)
+    got = rk.topk_rows(t, rows, workspace=ws, max_ctas=20)
+    t0, t1 = rk.call_span(ws)
+    assert 0 < t0 < t1 and t1 - t0 < 10**9  # nanoseconds of the GPU global timer
+    _check(x, rows, oo, got, False, "span call")

@@ -103,6 +103,27 @@ def test_parity_uneven_rows_and_idle_fill():
         assert_same_selection(got, want, lengths, [k] * len(lengths), [r * k for r in range(len(lengths))], sorted_)
 
 
+@pytest.mark.parametrize("shape", [(300, 32768, 64), (512, 5000, 100), (200, 20000, 3000), (64, 8192, 8192)])
+@pytest.mark.parametrize("dtype", [rk.F32, rk.F16])
+def test_calls_of_short_rows_only(shape, dtype):
+    # every row is selected by one team (smem or one-CTA rows): both the side
+    # and the consumer teams take rows, the consumer team in the ring
+    B, n, k = shape
+    flat = np.concatenate([values_for(dtype, n, "normal", 80 + r) for r in range(B)])
+    for largest, sorted_ in ((True, False), (False, True)):
+        got, want = run_both(flat, [n] * B, k, dtype, largest, sorted_)
+        assert_same_selection(got, want, [n] * B, [k] * B, [r * k for r in range(B)], sorted_)
+
+
+def test_uneven_short_rows_only():
+    lengths = [int(v) for v in workloads.rng(81).integers(1, 32768, size=300)]
+    flat = np.concatenate([values_for(rk.F32, n, "ties", 90 + r) for r, n in enumerate(lengths)])
+    k = 777
+    for sorted_ in (False, True):
+        got, want = run_both(flat, lengths, k, rk.F32, True, sorted_)
+        assert_same_selection(got, want, lengths, [k] * len(lengths), [r * k for r in range(len(lengths))], sorted_)
+
+
 @pytest.mark.parametrize("k", [2049, 4096, 5000, 8192])
 def test_sorted_short_rows_with_large_k(k):
     # rows held in shared memory (n <= 8192) whose sorted outputs exceed

@@ -136,7 +136,7 @@ struct alignas(16) Header {
   int64_t cand_total;   // candidate entries planned
   int64_t sort_total;   // sort-scratch entries planned
   int32_t fin_tail;     // FIN items at the end of the claim order
-  int32_t short_only;   // every row is selected by one team (nothing streams through the ring)
+  int32_t pad0;
   uint64_t t_first;     // %globaltimer (ns) when the engine's first CTA started
   uint64_t t_last;      // ... and when its last CTA ended
   int32_t pad[44];

@@ -2411,7 +2411,7 @@ __device__ __forceinline__ int claim_item(const EngineParams& p) {
 // copies of each streaming chunk into the ring as slots drain.
 template <int VT, bool SCALE>
 __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, int lag, int una, int unc, int ufin,
-                              int fin_tail, int first_q, bool short_only) {
+                              int fin_tail, int first_q) {
   constexpr int ES = KT<VT, SCALE>::ES, VEC = KT<VT, SCALE>::VEC;
   const int NQ = NA + NB;
   uint32_t g = 0, ci = 0, si = 0;
@@ -2473,15 +2473,7 @@ __device__ void producer_loop(const EngineParams& p, Ctrl* ctl, int NA, int NB, 
     if (!is_streaming(rc.kind, ir.isA, ir.fin)) {
       // Finishes in the tail of the claim order go to the consumer team (three
       // times the side team's threads): nothing streams after them.
-      bool to_cons = ir.fin && fin_tail > 0 && q >= NQ - fin_tail;
-      if (short_only && ir.isA && (rc.kind == kKindSmem || rc.kind == kKindCta)) {
-        // short rows go to the team with less queued work, counting the
-        // consumer team (24 warps) as three side teams (7 warps)
-        const uint32_t cq_load = ci - *reinterpret_cast<volatile uint32_t*>(&ctl->cons_done);
-        const uint32_t sq_load = si - *reinterpret_cast<volatile uint32_t*>(&ctl->side_done);
-        to_cons = cq_load <= 3u * sq_load;
-      }
-      if (to_cons) push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
+      if (ir.fin && fin_tail > 0 && q >= NQ - fin_tail) push(ctl->cq_full, ctl->cq_empty, ctl->cq, ci, d);
       else push(ctl->sq_full, ctl->sq_empty, ctl->sq, si, d);
       if (q + 1 >= NQ) {  // the last item: every later claim falls past the end
         q = NQ;
@@ -2609,16 +2601,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-// A short row (smem or one-CTA kind) on the consumer team, in a call that
-// streams nothing, so the ring is its scratch.  Not inlined: its registers
-// then do not weigh on the consumer team's streaming loop.
-template <int VT, bool SCALE>
-__device__ __noinline__ void cons_short_row(const EngineParams& p, uint8_t* smem, Misc* m, int r, const RowCtx& rc) {
-  Engine<VT, SCALE> er(p, smem, smem, m);
-  if (rc.kind == kKindSmem) er.template smem_row<ConsTeam>(r, rc);
-  else er.template cta_row<ConsTeam>(r, rc);
-}
-
 template <int VT, bool SCALE>
 __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __grid_constant__ EngineParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -2652,13 +2634,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   __syncthreads();
   int NA, NB, lag, fin_tail;
   int una = 1, unc = 0, ufin = 0;
-  // A call whose rows are all selected by one team each (smem and one-CTA
-  // rows) streams nothing through the ring: the consumer team then takes
-  // such rows too, with the ring as its scratch.
-  bool short_only;
   if (p.uniform) {
     const int kind = row_kind(p.u_n, p.u_k, p.cta_cap);
-    short_only = kind == kKindSmem || kind == kKindCta;
     una = row_na(kind, p.u_n, p.CH, p.CHR);
     unc = row_nbc(kind, p.u_n, p.CH, p.CHR);
     ufin = row_fin(kind);
@@ -2671,7 +2648,6 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
     NB = __ldcg(&p.hdr->nb);
     lag = __ldcg(&p.hdr->lag);
     fin_tail = __ldcg(&p.hdr->fin_tail);
-    short_only = __ldcg(&p.hdr->short_only) != 0;
   }
   // The CTA's first item is its block index.  A pre-filter sample taken here
   // is computed by the whole CTA before the teams start: nothing streams
@@ -2690,8 +2666,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   }
   const int warp = threadIdx.x >> 5;
   if (warp == kProducerWarp) {
-    if ((threadIdx.x & 31) == 0)
-      producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin, fin_tail, first_q, short_only);
+    if ((threadIdx.x & 31) == 0) producer_loop<VT, SCALE>(p, ctl, NA, NB, lag, una, unc, ufin, fin_tail, first_q);
   } else if (warp < kConsWarps) {
     // consumer team: streaming items
     Engine<VT, SCALE> e(p, smem, smem + kConsAreaOff, cons_misc(smem));
@@ -2722,8 +2697,6 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
         ConsTeam::sync();
         Engine<VT, SCALE> ef(p, smem, smem, m);
         ef.template fin_item_t<ConsTeam>(d.row, rc);
-      } else if (d.isA && (rc.kind == kKindSmem || rc.kind == kKindCta)) {
-        cons_short_row<VT, SCALE>(p, smem, m, d.row, rc);
       } else if (d.isA) {
         if (rc.kind == kKindAll) e.all_item(d.row, rc, d);
         else e.h_item(d.row, rc, d);

@@ -47,12 +47,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ int64_t run[5];
   __shared__ long long maxlag;
   __shared__ int has_radix;
-  __shared__ int has_stream;
   if (threadIdx.x < 5) run[threadIdx.x] = 0;
   if (threadIdx.x == 0) {
     maxlag = 0;
     has_radix = 0;
-    has_stream = 0;
   }
   __syncthreads();
   const bool sorted = (flags & kFlagSorted) != 0;
@@ -74,7 +72,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       cand = row_cand_cap(kind, d.n);
       hist = row_uses_hist(kind);
       if (kind == kKindGridRadix) has_radix = 1;
-      if (kind == kKindAll || kind == kKindGridPref || kind == kKindGridRadix) has_stream = 1;
       const int64_t kk = min((int64_t)d.n, (int64_t)d.k);
       sortn = (sorted && kk > kCapSort) ? 2 * kk : 0;
     }
@@ -120,7 +117,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     hdr->na = (int32_t)run[0];
     hdr->nb = (int32_t)nb_total;
     hdr->fin_tail = (int32_t)tail;
-    hdr->short_only = has_stream ? 0 : 1;
     hdr->cand_total = run[2];
     hdr->sort_total = run[3];
     hdr->plan_error = ok ? 0 : 1;

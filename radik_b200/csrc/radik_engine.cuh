@@ -2752,8 +2752,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
 
 // coop = false launches the same grid without the cooperative attribute: for
 // a grid below the device's, whose caller keeps the grids of concurrent
-// launches within the SM count (every CTA then finds a free SM); cooperative
-// launches of the engine did not run side by side on a B200.
+// launches within the SM count, so every CTA finds a free SM.
 template <int VT, bool SCALE>
 inline cudaError_t launch_typed(const EngineParams& p, int grid, cudaStream_t stream, bool coop = true) {
   auto kern = dev::engine_kernel<VT, SCALE>;

@@ -1246,21 +1246,30 @@ struct Engine {
       }
       if (ConsTeam::tid() == 0) RADIK_TL_ACC(p, kTlAccFull, tw);
       const uint4* st = ring + slot * kStageVecs;
+      // The warp's vectors of the stage are read into registers, then the
+      // slot is released before they are processed: a warp that meets hits
+      // (the compaction is the slow path) no longer holds the refill of the
+      // slot for every other warp.
+      uint4 v[kPer];
       if (i < nfull) {
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) fv(st[j * ConsTeam::kSize], pos + (int64_t)j * ConsTeam::kSize * VEC, true);
+        for (int j = 0; j < kPer; ++j) v[j] = st[j * ConsTeam::kSize];
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) fv(v[j], pos + (int64_t)j * ConsTeam::kSize * VEC, true);
       } else {
         const int cnt = (int)(d.nvec - (int64_t)i * kStageVecs);
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-          const bool ok = j * ConsTeam::kSize + ConsTeam::tid() < cnt;
-          const uint4 x = ok ? st[j * ConsTeam::kSize] : make_uint4(0, 0, 0, 0);
-          fv(x, pos + (int64_t)j * ConsTeam::kSize * VEC, ok);
-        }
+        for (int j = 0; j < kPer; ++j)
+          v[j] = j * ConsTeam::kSize + ConsTeam::tid() < cnt ? st[j * ConsTeam::kSize] : make_uint4(0, 0, 0, 0);
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
+#pragma unroll
+        for (int j = 0; j < kPer; ++j)
+          fv(v[j], pos + (int64_t)j * ConsTeam::kSize * VEC, j * ConsTeam::kSize + ConsTeam::tid() < cnt);
       }
       pos += (int64_t)kStageVecs * VEC;
-      __syncwarp();
-      if ((threadIdx.x & 31) == 0) mbar_arrive(&ctl->empty[slot]);
       if (++slot == NS) {
         slot = 0;
         parity ^= 1u;

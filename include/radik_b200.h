@@ -225,7 +225,8 @@ int radik_shard_collect(int dtype, uint32_t flags, const void* val_in, int64_t n
  * row already on the device; its results land in the request's own device
  * buffers.  Requests that arrive while batches run are admitted into the next
  * batch as a slot, the budget and free SMs allow: a batch asks for one engine
- * CTA (one SM) per 2^16 keys, at most three quarters of the device when
+ * CTA (one SM) per 2^16 keys (at least 32 when no other batch is in flight),
+ * at most three quarters of the device when
  * several slots exist, and starts when that many SMs are free of other
  * batches.  So several batches are in flight at once and their selection
  * kernels run side by side on disjoint SMs.  Each

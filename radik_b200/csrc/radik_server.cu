@@ -13,8 +13,9 @@
 //
 // SMs are the third resource a batch is admitted by, beside its slot and the
 // memory budget: the engine runs one CTA per SM, so a batch asks for one CTA
-// per 2^16 keys (at most three quarters of the device when several slots
-// exist) and starts only when that many SMs are free of other batches.  The
+// per 2^16 keys (at least 32 on an idle device) and at most three quarters
+// of the device when several slots exist, and starts only when that many SMs
+// are free of other batches.  The
 // engines of concurrent batches therefore sit on disjoint SMs and run side by
 // side: a batch of small requests does not wait for a large one to finish.
 //
@@ -97,7 +98,13 @@ struct Slot {
 
 // Keys per engine CTA a batch asks for.  At 2^16 fp32 keys (256 KB) a CTA
 // streams its share in a few microseconds, about the engine's fixed cost.
+// A batch that finds no other batch in flight takes at least kIdleBatchCtas:
+// a row of 128K keys on two CTAs streams for longer than the engine's fixed
+// cost.  Under load it takes only its share, so that small batches never
+// hold the SMs a large one is waiting for (a floor of 16 CTAs for every batch
+// raised p99 at 50k requests/s from 0.50 to 1.49 ms).
 constexpr int64_t kKeysPerCta = (int64_t)1 << 16;
+constexpr int kIdleBatchCtas = 32;
 
 }  // namespace
 
@@ -172,7 +179,8 @@ struct Server {
 
   // Engine CTAs a batch of `keys` keys asks for.
   int want_ctas(int64_t keys) const {
-    const int64_t w = (keys + kKeysPerCta - 1) / kKeysPerCta;
+    int64_t w = (keys + kKeysPerCta - 1) / kKeysPerCta;
+    if (ctas_inflight == 0) w = std::max<int64_t>(w, kIdleBatchCtas);
     return (int)std::max<int64_t>(1, std::min<int64_t>(w, ctas_cap));
   }
 

@@ -22,6 +22,7 @@
 namespace radik {
 
 cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream, bool coop = true);
+cudaError_t launch_short_rows(int dtype, const EngineParams& p, int grid, cudaStream_t stream);
 cudaError_t launch_plan(const RowDesc* desc, int B, int CH, int CHR, int cta_cap, int D, uint32_t flags,
                         RowPlan* plans, int32_t* a_row, int32_t* b_row, Header* hdr, int64_t na_cap, int64_t nb_cap,
                         int64_t cand_cap_total, int64_t sort_cap_total, int grid, cudaStream_t stream);
@@ -415,6 +416,14 @@ int launch_call(int dtype, uint32_t flags, const void* val_in, const void* idx_i
     p.u_cand_cap = row_cand_cap(kind, n);
     const int64_t kk = std::min<int64_t>(n, K);
     p.u_sort_cap = ((flags & kFlagSorted) && kk > kCapSort) ? 2 * kk : 0;
+    if (kind == kKindSmem || kind == kKindCta) {
+      // every row is one team's work: the short-row kernel, four teams a CTA
+      // (4096 x 32768 keys, k = 64: 0.92 ms on the engine's side teams)
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (B + 3) / 4));
+      e = launch_short_rows(dtype, p, g, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "short-row launch");
+      return RADIK_OK;
+    }
     // B sequence layout (see UniformB) and the lag it needs
     const int64_t una = row_na(kind, n, cfg.CH, cfg.CHR), nc = row_nbc(kind, n, cfg.CH, cfg.CHR);
     const int64_t f = row_fin(kind);

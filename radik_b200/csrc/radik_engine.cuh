@@ -2757,7 +2757,74 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
   }
 }
 
+// ----------------------------------------------------------------------------
+// Short-row kernel: equal-length calls whose rows are each selected by one team
+// (smem rows, n <= 8192, or one-CTA rows, n <= cta_cap).  No row needs the
+// grid, so nothing streams through a ring and no CTA waits for another: four
+// 256-thread teams per CTA each claim whole rows from the call's counter and
+// select them with the side team's code, each in a side-sized area of its own.
+// In the engine these rows run on the 7-warp side team alone.
+// ----------------------------------------------------------------------------
+constexpr int kRowTeams = 4;
+constexpr int kRowTeamThreads = kThreads / kRowTeams;
+constexpr int kRowMiscOff = kRowTeams * kSideAreaBytes;
+constexpr int kShortSmemBytes = kRowMiscOff + kRowTeams * 3072;
+static_assert(kShortSmemBytes <= 227 * 1024, "short-row kernel smem");
+
+template <int VT, bool SCALE, int T>
+__device__ __forceinline__ void row_team_loop(const EngineParams& p, uint8_t* smem) {
+  using Tm = TeamT<T * kRowTeamThreads, kRowTeamThreads, 3 + T>;
+  Misc* m = reinterpret_cast<Misc*>(smem + kRowMiscOff + T * 3072);
+  Engine<VT, SCALE> e(p, smem, smem + T * kSideAreaBytes, m);
+  for (;;) {
+    if (Tm::tid() == 0) m->bcast = (int)atomicAdd(&p.hdr->qhead, 1u);
+    Tm::sync();
+    const int r = m->bcast;
+    Tm::sync();
+    if (r >= p.B) break;
+    const RowCtx rc = load_row<VT, SCALE>(p, r);
+    if (rc.kind == kKindSmem) e.template smem_row<Tm>(r, rc);
+    else if (rc.kind == kKindCta) e.template cta_row<Tm>(r, rc);
+    Tm::sync();
+  }
+}
+
+template <int VT, bool SCALE>
+__global__ void __launch_bounds__(kThreads, 1) short_rows_kernel(const __grid_constant__ EngineParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  if (threadIdx.x == 0)
+    atomicCAS(reinterpret_cast<unsigned long long*>(&p.hdr->t_first), 0ull, globaltimer_ns());
+  switch (threadIdx.x / kRowTeamThreads) {
+    case 0: row_team_loop<VT, SCALE, 0>(p, smem); break;
+    case 1: row_team_loop<VT, SCALE, 1>(p, smem); break;
+    case 2: row_team_loop<VT, SCALE, 2>(p, smem); break;
+    default: row_team_loop<VT, SCALE, 3>(p, smem); break;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(reinterpret_cast<unsigned long long*>(&p.hdr->t_last), globaltimer_ns());
+}
+
 }  // namespace dev
+
+template <int VT, bool SCALE>
+inline cudaError_t launch_short_typed(const EngineParams& p, int grid, cudaStream_t stream) {
+  auto kern = dev::short_rows_kernel<VT, SCALE>;
+  static std::mutex attr_mu;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lock(attr_mu);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dev::kShortSmemBytes);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+  }
+  kern<<<grid, kThreads, dev::kShortSmemBytes, stream>>>(p);
+  return cudaGetLastError();
+}
 
 // coop = false launches the same grid without the cooperative attribute: for
 // a grid below the device's, whose caller keeps the grids of concurrent
@@ -2807,6 +2874,9 @@ inline cudaError_t engine_occupancy(int* per_sm) {
 
 // Per value type entry points (one translation unit each).
 cudaError_t launch_engine_f32(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
+cudaError_t launch_short_f32(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_short_f16(const EngineParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_short_bf16(const EngineParams& p, int grid, cudaStream_t stream);
 cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
 cudaError_t launch_engine_bf16(const EngineParams& p, int grid, cudaStream_t stream, bool coop);
 cudaError_t occupancy_f32(uint32_t flags, int* per_sm);

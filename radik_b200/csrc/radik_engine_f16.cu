@@ -9,6 +9,11 @@ cudaError_t launch_engine_f16(const EngineParams& p, int grid, cudaStream_t stre
                                     : launch_typed<kF16, false>(p, grid, stream, coop);
 }
 
+cudaError_t launch_short_f16(const EngineParams& p, int grid, cudaStream_t stream) {
+  return (p.flags & kFlagWithScale) ? launch_short_typed<kF16, true>(p, grid, stream)
+                                    : launch_short_typed<kF16, false>(p, grid, stream);
+}
+
 cudaError_t occupancy_f16(uint32_t flags, int* per_sm) {
   return (flags & kFlagWithScale) ? engine_occupancy<kF16, true>(per_sm) : engine_occupancy<kF16, false>(per_sm);
 }

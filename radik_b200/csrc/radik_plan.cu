@@ -161,6 +161,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 }  // namespace dev
 
+cudaError_t launch_short_rows(int dtype, const EngineParams& p, int grid, cudaStream_t stream) {
+  switch (dtype) {
+    case kF32: return launch_short_f32(p, grid, stream);
+    case kF16: return launch_short_f16(p, grid, stream);
+    case kBF16: return launch_short_bf16(p, grid, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_engine(int dtype, const EngineParams& p, int grid, cudaStream_t stream, bool coop) {
   switch (dtype) {
     case kF32: return launch_engine_f32(p, grid, stream, coop);

@@ -331,6 +331,7 @@ int fin_delay_uniform(int nc, int grid) { return std::max(1, (3 * grid + 2 * std
 struct CallPlan {
   int B = 0, grid = 0;
   bool uniform = true, has_radix = false;
+  bool short_only = true;  // every row is a smem or one-CTA row (one team's work)
   Config cfg{};
   int64_t na = 0, nb = 0, cand = 0, sortn = 0;
   Layout L{};
@@ -360,11 +361,12 @@ int plan_call(int dtype, uint32_t flags, const int* task_len, int task_num, int 
   }
   const Config cfg = choose_config(multi_elems, grid, t, (int)elem_bytes(dtype), uniform ? n_max : 0, B);
   int64_t na = 0, nb = 0, cand = 0, sortn = 0;
-  bool has_radix = false;
+  bool has_radix = false, short_only = true;
   for (int i = 0; i < B; ++i) {
     const int n = task_len[i];
     const int kind = row_kind(n, K, cta_cap);
     has_radix = has_radix || kind == kKindGridRadix;
+    short_only = short_only && (kind == kKindSmem || kind == kKindCta);
     na += row_na(kind, n, cfg.CH, cfg.CHR);
     nb += row_nbc(kind, n, cfg.CH, cfg.CHR) + row_fin(kind);
     cand += row_cand_cap(kind, n);
@@ -376,6 +378,7 @@ int plan_call(int dtype, uint32_t flags, const int* task_len, int task_num, int 
   cp->grid = grid;
   cp->uniform = uniform;
   cp->has_radix = has_radix;
+  cp->short_only = short_only;
   cp->cfg = cfg;
   cp->na = na;
   cp->nb = nb;
@@ -472,6 +475,14 @@ int launch_call(int dtype, uint32_t flags, const void* val_in, const void* idx_i
                     reinterpret_cast<int32_t*>(ws + L.a_row), reinterpret_cast<int32_t*>(ws + L.b_row), p.hdr, cp.na,
                     cp.nb, cp.cand, cp.sortn, grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "plan launch");
+    if (cp.short_only) {
+      // rows of unequal length, each one team's work: the short-row kernel
+      // reads them from the plans
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (B + 3) / 4));
+      e = launch_short_rows(dtype, p, g, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "short-row launch");
+      return RADIK_OK;
+    }
   }
   e = launch_engine(dtype, p, grid, stream);
   if (e != cudaSuccess) return cuda_fail(e, "engine launch");

@@ -2758,8 +2758,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM) engine_kernel(const __gr
 }
 
 // ----------------------------------------------------------------------------
-// Short-row kernel: equal-length calls whose rows are each selected by one team
-// (smem rows, n <= 8192, or one-CTA rows, n <= cta_cap).  No row needs the
+// Short-row kernel: calls whose rows are each selected by one team (smem
+// rows, n <= 8192, or one-CTA rows, n <= cta_cap), of equal length or, with
+// the planning kernel run first, of lengths known on the host.  No row needs the
 // grid, so nothing streams through a ring and no CTA waits for another: four
 // 256-thread teams per CTA each claim whole rows from the call's counter and
 // select them with the side team's code, each in a side-sized area of its own.
@@ -2792,6 +2793,7 @@ __device__ __forceinline__ void row_team_loop(const EngineParams& p, uint8_t* sm
 template <int VT, bool SCALE>
 __global__ void __launch_bounds__(kThreads, 1) short_rows_kernel(const __grid_constant__ EngineParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
+  if (!p.uniform && __ldcg(&p.hdr->plan_error)) return;
   if (threadIdx.x == 0)
     atomicCAS(reinterpret_cast<unsigned long long*>(&p.hdr->t_first), 0ull, globaltimer_ns());
   switch (threadIdx.x / kRowTeamThreads) {

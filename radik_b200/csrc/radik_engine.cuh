@@ -342,8 +342,11 @@ constexpr int kCapTail = 16384;  // candidates a tail finish on the consumer tea
 static_assert(kCapTail * 8 + 1024 <= kRingBytes && 32768 * 4 + 1024 <= kRingBytes, "ring as scratch");
 constexpr int kSideCandMax = 1 << 17;  // candidate sets the side team resolves itself (else phase B)
 // Batches of fewer rows leave the grid idle at their end, so there every set
-// too large for smem goes to phase B, which resolves it with all CTAs.
+// too large for smem goes to phase B, which resolves it with all CTAs --
+// except sets of up to kTailResolveMax in a finish on the consumer team,
+// which resolves them from L2 itself in less time than phase B's barriers.
 constexpr int kSideResolveMinRows = 32;
+constexpr int kTailResolveMax = 1 << 15;
 
 struct Ctrl {
   uint64_t full[kStages];   // ring slot filled
@@ -2053,7 +2056,8 @@ struct Engine {
         if (Tm::tid() == 0) RADIK_TL(p, kTlFinEmitted);
         post_process<Tm, VT, SCALE>(p, rc, smem, m);
         if (Tm::tid() == 0) RADIK_TL(p, kTlFinPost);
-      } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax) && p.B >= kSideResolveMinRows) {
+      } else if (c >= rc.k && c <= min(rc.cand_cap, kSideCandMax) &&
+                 (p.B >= kSideResolveMinRows || (Tm::kSize == ConsTeam::kSize && c <= kTailResolveMax))) {
         side_cand_resolve<Tm>(r, rc, c, 0, 0, rc.k, c);
       } else if (c >= rc.k && c <= rc.cand_cap) {
         to_phase_b<Tm>(r, 1, c, 0, 0, rc.k, c);
